@@ -1,0 +1,373 @@
+"""Benchmark of the XXZ Lanczos ground-state path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Metric (the reference project's headline): H*v/s and HBM GB/s, mixed vs FP64
+at |dE0| < 1e-9; batched sectors/s.  A "step" is one complete ground-state
+solve of the workload.  Workloads (synthetic, seeded):
+
+  batched (default)  256 XXZ chains L=20, periodic, Delta ~ U(0,2), J ~ U(0.5,1.5)
+                     (mt19937-64 seed 20261203), every momentum sector k=0..19 of Sz=0,
+                     one batched mixed-precision Lanczos (FP32 vectors/values, FP64
+                     scalars, FP64 refinement restart)
+  l24                L=24 XXZ chain, J=1, Delta=0.5, k=0, spin-inversion even (56,450 rows),
+                     mixed precision
+  l16                L=16 Heisenberg chain, full Sz=0 sector, FP64, 150 steps, full
+                     reorthogonalisation
+  l32                L=32 J1-J2 chain (1, 0.5), Delta=1, k=0, even, FP32 vectors with FP64
+                     reductions + refinement, 300 steps max, matrix-free H*v optional
+
+`value` counts sector H*v products (one coupling set x one sector x one
+product) per second of device time with inputs resident; `e2e` is the same
+count over the wall time of the public C-ABI calls from host buffers (sector
+build, matrix build, solve, result copy).  `--impl reference` times the
+reference's own CPU H*v (SparseMatDenseVec_prod_EEL_host, compiled from its
+sources into oracle/_ref) on the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Hv/s and HBM GB/s, mixed vs FP64 at |dE0|<1e-9; batched sectors/s"
+SEED = 20261203
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def couplings(n_sets: int, rank: int = 0):
+    """Delta_i ~ U(0,2), J_i ~ U(0.5,1.5) from mt19937-64(seed), drawn in set order."""
+    rng = np.random.Generator(np.random.MT19937(SEED + rank))
+    d = np.empty(n_sets)
+    j = np.empty(n_sets)
+    for i in range(n_sets):
+        d[i] = rng.uniform(0.0, 2.0)
+        j[i] = rng.uniform(0.5, 1.5)
+    return j, d
+
+
+class Clocks:
+    """nvidia-smi clock sampling during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
+        except OSError:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[3:7]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)
+
+
+# --------------------------------------------------------------- workloads
+def build_batched(q, L=20, n_sets=256):
+    perm, ch = q.translation_group(L)
+    secs = [q.Sector(L, L // 2, perm).set_irrep(ch[a]) for a in range(L)]
+    bonds = q.chain_bonds(L)
+    b = q.Batch(secs, q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"),
+                n_sets)
+    return secs, b
+
+
+def time_batch_hv(torch, q, b, prec, reps=20):
+    """Average device time of one batched H*v (CUDA events on the launch stream)."""
+    off, cp = b.layout()
+    tot = int(off[-1])
+    dt = torch.float64 if prec == q._capi.PREC_FP64 else torch.float32
+    x = torch.randn(tot, dtype=dt, device="cuda")
+    y = torch.empty_like(x)
+    st = torch.cuda.current_stream()
+    sh = st.cuda_stream
+    for _ in range(3):
+        b.hv_dev(x.data_ptr(), y.data_ptr(), prec, sh)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(reps):
+        b.hv_dev(x.data_ptr(), y.data_ptr(), prec, sh)
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_batched(args, torch, q, rank, world):
+    A = q._capi
+    L, n_sets = 20, 256
+    J, D = couplings(n_sets, rank)
+    secs, b = build_batched(q, L, n_sets)
+    info = b.info
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device="cuda")
+    opts = dict(mode=A.MODE_MIXED, max_iter=300, tol=1e-12, check_every=10, refine_max_iter=60,
+                seed=SEED)
+
+    def solve(mode):
+        o = dict(opts, mode=mode)
+        return b.solve(J, J * D, **o)
+
+    for _ in range(args.warmup):
+        solve(A.MODE_MIXED)
+    torch.cuda.synchronize()
+    dev_ms, hv_count = [], []
+    with Clocks(torch.cuda.current_device()) as clk:
+        for _ in range(args.steps):
+            flush_l2(torch, flush)
+            torch.cuda.synchronize()
+            E_mix, r = solve(A.MODE_MIXED)
+            dev_ms.append(r.ms_total)
+            hv_count.append(r.n_hv)
+    clocks = clk.summary()
+    # FP64 reference solve of the same problems, |dE0| of the mixed result
+    E64, r64 = solve(A.MODE_FP64)
+    rel = np.abs(E_mix - E64) / np.maximum(np.abs(E64), 1e-300)
+    # per-kernel H*v times
+    hv32_ms = time_batch_hv(torch, q, b, A.PREC_FP32)
+    hv64_ms = time_batch_hv(torch, q, b, A.PREC_FP64)
+    units = n_sets * L  # sector problems per batched H*v
+    ms = float(np.mean(dev_ms))
+    value = float(np.mean(hv_count)) * units / (ms * 1e-3)
+    # end-to-end through the C ABI from host buffers: sectors, batch, solve
+    e2e_t = []
+    for _ in range(max(1, min(3, args.steps))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2, b2 = build_batched(q, L, n_sets)
+        E2, r2 = b2.solve(J, J * D, **opts)
+        t1 = time.perf_counter()
+        e2e_t.append(t1 - t0)
+        b2.close()
+        for s in s2:
+            s.close()
+    e2e_s = float(np.mean(e2e_t))
+    out = {
+        "workload": "batched: 256 XXZ chains L=20 periodic, Delta~U(0,2), J~U(0.5,1.5) "
+                    "(mt19937-64 seed 20261203), all k=0..19 of Sz=0, mixed precision",
+        "n_sets": n_sets, "L": L, "sectors": L, "problems": units,
+        "rows_total": int(info.rows_total), "elements_per_hv": int(info.elems_total),
+        "l2_policy": "vectors per batched H*v > L2 (FP32 %.0f MB); 256 MB written between steps"
+                     % (info.bytes_hv_fp32 / 1e6),
+        "parallelism": f"dp{world} (independent coupling sets per GPU)",
+    }
+    extra = {
+        "sectors_per_s": units / (ms * 1e-3),
+        "hv_per_solve": float(np.mean(hv_count)),
+        "fp64_solve_ms": r64.ms_total, "fp64_hv_per_s": r64.n_hv * units / (r64.ms_total * 1e-3),
+        "hv_kernel_ms_fp32": hv32_ms, "hv_kernel_ms_fp64": hv64_ms,
+        "hv_kernel_gbs_fp32": info.bytes_hv_fp32 / (hv32_ms * 1e-3) / 1e9,
+        "hv_kernel_gbs_fp64": info.bytes_hv_fp64 / (hv64_ms * 1e-3) / 1e9,
+        "hv_ratio_fp32_over_fp64": hv64_ms / hv32_ms,
+        "max_rel_dE0_mixed_vs_fp64": float(rel.max()),
+        "E0_min": float(E_mix.min()),
+    }
+    roof_bytes = info.bytes_hv_fp32
+    return dict(ms=ms, value=value, units_per_step=float(np.mean(hv_count)) * units, out=out,
+                extra=extra, clocks=clocks, e2e_s=e2e_s,
+                e2e_value=float(np.mean(hv_count)) * units / e2e_s,
+                h2d=2 * n_sets * 8, d2h=n_sets * L * 8, roof_bytes=roof_bytes, roof_ms=hv32_ms,
+                launches=int(np.mean(hv_count)) * 5, kernel="k_bhv<float2,8> (batched H*v, FP32)",
+                dtype="f32+f64")
+
+
+def reference_tables(L=20, n_sets_sample=2):
+    """Reference-layout FP32 ELLs of the batched workload built by the
+    reference's own kernels (oracle/_ref, emulated on the host)."""
+    import oracle as O
+    import qmbcuda_b200 as q
+    R = O.ref()
+    perm, ch = q.translation_group(L)
+    k = L // 2
+    N = O.binom(L, k)
+    G = L
+    reps = np.zeros(N, np.uint32)
+    srs = np.zeros(N * G, np.uint32)
+    norms = np.zeros(N * G, np.float32)
+    oi = np.zeros(2 * N, np.uint32)
+    chf = np.ascontiguousarray(ch.astype(np.complex64)).view(np.float32).ravel()
+    Rn = R.ref_build_srs_complex(L, k, G, np.ascontiguousarray(perm), G, chf, reps, N, srs, norms, oi)
+    J, D = couplings(n_sets_sample)
+    tabs = []
+    bonds = q.chain_bonds(L)
+    W = 2 * L + 1
+    for i in range(n_sets_sample):
+        t = q.xxz_terms(bonds, J[i], J[i] * D[i])
+        codes = np.ascontiguousarray(t.codes.ravel(), np.int32)
+        sites = np.ascontiguousarray(t.sites.ravel(), np.int32)
+        sc = np.ascontiguousarray(t.scalar.astype(np.complex64)).view(np.float32).ravel()
+        for a in range(L):
+            ind = np.zeros(Rn * W, np.uint32)
+            val = np.zeros(2 * Rn * W, np.float32)
+            tr = np.zeros(Rn, np.int16)
+            R.ref_ham_terms_complex(L, k, G, Rn, srs, oi, G, chf, a, norms, 1e-5, t.n_terms, 2,
+                                    t.n_ops, codes, sites, sc, W, ind, val, tr)
+            tabs.append((ind, val, tr, Rn, W))
+    return tabs
+
+
+def cpu_reference_hv(seconds=10.0, threads=None):
+    """The reference's CPU H*v (FP32 float path of SparseMatDenseVec_prod_EEL_host)
+    on the batched workload's sector matrices; complex sectors are timed on their
+    real part, which has the same index traffic (the reference's host H*v is
+    float-only).  Returns (Hv/s, threads, sample description)."""
+    import oracle as O
+    R = O.ref()
+    threads = threads or os.cpu_count() or 1
+    tabs = reference_tables()
+    xs = [np.random.default_rng(i).standard_normal(t[3]).astype(np.float32) for i, t in enumerate(tabs)]
+    reals = [np.ascontiguousarray(t[1].reshape(-1, 2)[:, 0]) for t in tabs]
+    ys = [np.zeros(t[3], np.float32) for t in tabs]
+    # warm
+    for (ind, val, tr, n, W), vr, x, y in zip(tabs, reals, xs, ys):
+        R.ref_spmv_host(ind, vr, tr, x, y, n, W, threads)
+    count = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        for (ind, val, tr, n, W), vr, x, y in zip(tabs, reals, xs, ys):
+            R.ref_spmv_host(ind, vr, tr, x, y, n, W, threads)
+            count += 1
+    dt = time.perf_counter() - t0
+    return count / dt, threads, f"{len(tabs)} sector matrices (2 coupling sets x 20 k) of L=20, " \
+                                f"{count} H*v in {dt:.1f} s"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="batched", choices=["batched"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        v, thr, sample = cpu_reference_hv(args.cpu_seconds)
+        line = {"metric": METRIC, "value": v, "unit": "Hv/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "batched: 256 XXZ chains L=20, all k, reference CPU H*v sample",
+                           "parallelism": "host threads"},
+                "cpu_baseline": {"value": v, "unit": "Hv/s", "cores": thr, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "Hv/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import qmbcuda_b200 as q
+
+    if dist:
+        dist.barrier()
+    res = run_batched(args, torch, q, rank, world)
+    ms = res["ms"]
+    if dist:
+        t = torch.tensor([ms, res["e2e_s"]], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(t[0]), float(t[1])
+    else:
+        e2e_s = res["e2e_s"]
+    total_units = res["units_per_step"] * world
+    value = total_units / (ms * 1e-3)
+    peak, peak_kind = load_peaks()
+    achieved = res["roof_bytes"] / (res["roof_ms"] * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "batched_hv_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("traffic_bytes_per_launch")
+    line = {
+        "metric": METRIC, "value": value, "unit": "Hv/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": res["dtype"], "data": "synthetic", "config": res["out"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": res["kernel"],
+                     "peak_source": peak_kind},
+        "e2e": {"value": total_units / e2e_s, "unit": "Hv/s",
+                "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
+        "clocks": res["clocks"], "gpu_launches": res["launches"],
+    }
+    line.update(res["extra"])
+    if rank == 0 and world == 1:
+        try:
+            v, thr, sample = cpu_reference_hv(args.cpu_seconds)
+            line["cpu_baseline"] = {"value": v, "unit": "Hv/s", "cores": thr, "kind": "reference",
+                                    "sample": sample}
+        except Exception as e:  # reference build absent
+            line["cpu_baseline"] = {"value": None, "unit": "Hv/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,141 @@
+// qmb_group.cuh -- group-element application on device.
+#pragma once
+#include "qmb_common.cuh"
+
+namespace qmb {
+
+// One site map as word operations (structured groups).
+struct ElemRot {
+    uint64_t lo;  // bits moved up by the in-row rotation
+    uint32_t rr;  // whole-word rotation (bits)
+    uint32_t ri;  // in-row rotation (bits)
+};
+
+constexpr int kMaxPerm = 512;        // site maps per group
+constexpr int kTableSmemMax = 96 * 1024;
+
+// Group description handed to kernels by value.
+struct GroupArgs {
+    int L, G, n_ext, structured, W, n_chunks;
+    uint64_t mask;
+    const ElemRot* rot;       // [G] device
+    const uint64_t* tables;   // [G][n_chunks][16] device
+    const double2* chars;     // [n_ext] device (selected irrep), may be null
+};
+
+// Shared-memory copy of the group, loaded by every thread block.
+struct GroupSmem {
+    const ElemRot* rot;
+    const uint64_t* tab;
+};
+
+// Bytes of dynamic shared memory a kernel needs for the group.
+__host__ __device__ inline size_t group_smem_bytes(const GroupArgs& g) {
+    if (g.structured) return sizeof(ElemRot) * (size_t)g.G;
+    size_t t = sizeof(uint64_t) * (size_t)g.G * g.n_chunks * 16;
+    return t <= (size_t)kTableSmemMax ? t : 0;
+}
+
+// Cooperative load of the group into dynamic shared memory `sm`.
+__device__ __forceinline__ GroupSmem load_group(const GroupArgs& g, unsigned char* sm) {
+    GroupSmem out;
+    if (g.structured) {
+        ElemRot* r = reinterpret_cast<ElemRot*>(sm);
+        for (int i = threadIdx.x; i < g.G; i += blockDim.x) r[i] = g.rot[i];
+        out.rot = r;
+        out.tab = g.tables;
+    } else {
+        size_t n = (size_t)g.G * g.n_chunks * 16;
+        if (n * sizeof(uint64_t) <= (size_t)kTableSmemMax) {
+            uint64_t* t = reinterpret_cast<uint64_t*>(sm);
+            for (size_t i = threadIdx.x; i < n; i += blockDim.x) t[i] = g.tables[i];
+            out.tab = t;
+        } else {
+            out.tab = g.tables;
+        }
+        out.rot = g.rot;
+    }
+    __syncthreads();
+    return out;
+}
+
+// Image of s under site map g (no inversion).
+__device__ __forceinline__ uint64_t apply_site_map(const GroupArgs& g, const GroupSmem& sm, int gi,
+                                                   uint64_t s) {
+    if (g.structured) {
+        ElemRot e = sm.rot[gi];
+        uint64_t y = rotl_bits(s, (int)e.rr, g.L, g.mask);
+        return rot_rows(y, (int)e.ri, g.W, e.lo);
+    }
+    const uint64_t* t = sm.tab + (size_t)gi * g.n_chunks * 16;
+    uint64_t y = 0;
+#pragma unroll 4
+    for (int c = 0; c < g.n_chunks; ++c) y |= t[c * 16 + (int)((s >> (4 * c)) & 15ull)];
+    return y;
+}
+
+// Image under extended element e = z*G + g.
+__device__ __forceinline__ uint64_t apply_elem(const GroupArgs& g, const GroupSmem& sm, int e,
+                                               uint64_t s) {
+    int z = e >= g.G;
+    int gi = z ? e - g.G : e;
+    uint64_t y = apply_site_map(g, sm, gi, s);
+    return z ? (y ^ g.mask) : y;
+}
+
+// True iff no element maps s below s (s is its orbit's minimum).
+__device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, uint64_t s) {
+    for (int gi = 0; gi < g.G; ++gi) {
+        uint64_t y = apply_site_map(g, sm, gi, s);
+        if (y < s) return false;
+        if (g.n_ext > g.G && (y ^ g.mask) < s) return false;
+    }
+    return true;
+}
+
+// Minimum of the orbit of t and the first element reaching it.
+__device__ __forceinline__ uint64_t orbit_min(const GroupArgs& g, const GroupSmem& sm, uint64_t t,
+                                              int* elem) {
+    uint64_t best = t;
+    int be = 0;
+    bool flip = g.n_ext > g.G;
+    for (int gi = 0; gi < g.G; ++gi) {
+        uint64_t y = apply_site_map(g, sm, gi, t);
+        if (y < best) { best = y; be = gi; }
+        if (flip) {
+            uint64_t yz = y ^ g.mask;
+            if (yz < best) { best = yz; be = gi + g.G; }
+        }
+    }
+    // element 0 is checked first above; if t itself is minimal and element 0
+    // is not the identity, find an element that fixes t.
+    if (be == 0 && best == t && apply_site_map(g, sm, 0, t) != t) {
+        for (int e = 1; e < g.n_ext; ++e)
+            if (apply_elem(g, sm, e, t) == t) { be = e; break; }
+    }
+    *elem = be;
+    return best;
+}
+
+// Orbit index of representative r in the sorted table, or -1.  bucket[b]
+// holds the first table position whose string has top bits >= b.
+struct RepTable {
+    const uint64_t* reps;
+    const uint32_t* bucket;  // [2^T + 1]
+    int64_t R;
+    int shift;               // L - T
+};
+
+__device__ __forceinline__ int64_t find_rep(const RepTable& t, uint64_t r) {
+    uint64_t b = r >> t.shift;
+    int64_t lo = t.bucket[b], hi = t.bucket[b + 1];
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        uint64_t v = __ldg(t.reps + mid);
+        if (v < r) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < t.R && t.reps[lo] == r) ? lo : -1;
+}
+
+}  // namespace qmb

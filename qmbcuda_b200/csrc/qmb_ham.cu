@@ -1,0 +1,427 @@
+// qmb_ham.cu -- symmetric-basis XXZ matrix on the GPU.
+//
+// Builds the matrix of the active rows of a sector's irrep from operator
+// tables with the rule of BuildHamiltonianXXZForAbelianGroup
+// (exact_diagonalization/utils.cu:83-184), into a sliced ELL layout: rows in
+// 32-row slices, slot j of the slice stored contiguously for its 32 rows, so
+// a warp's loads of one slot are one coalesced 128-byte (FP32) / 256-byte
+// (FP64) transaction.  Slice width = longest row of the slice.  The diagonal
+// is a separate dense vector.  Two passes: count entries per row, then fill.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "qmb_ham.cuh"
+
+namespace qmb {
+
+void upload_terms(qmb_ham_s* h, const qmb_terms* t, int L) {
+    QMB_REQUIRE(t && t->n_ops && t->op_code && t->op_site && t->scalar, QMB_ERR_INVALID,
+                "terms: null table");
+    QMB_REQUIRE(t->n_terms >= 0 && t->n_terms <= kMaxTerms, QMB_ERR_INVALID,
+                "terms: n_terms must be in 0..4096");
+    QMB_REQUIRE(t->n_col >= 1 && t->n_col <= kMaxCol, QMB_ERR_INVALID,
+                "terms: n_col must be in 1..8");
+    std::vector<int> nops(t->n_terms);
+    std::vector<uint16_t> ops((size_t)t->n_terms * t->n_col, 0);
+    std::vector<double2> sc(t->n_terms);
+    for (int i = 0; i < t->n_terms; ++i) {
+        QMB_REQUIRE(t->n_ops[i] >= 0 && t->n_ops[i] <= t->n_col, QMB_ERR_INVALID,
+                    "terms: n_ops out of range");
+        nops[i] = t->n_ops[i];
+        for (int j = 0; j < t->n_ops[i]; ++j) {
+            int c = t->op_code[i * t->n_col + j], s = t->op_site[i * t->n_col + j];
+            QMB_REQUIRE(c >= 0 && c <= 255, QMB_ERR_INVALID, "terms: op code out of range");
+            QMB_REQUIRE(s >= 0 && s < L, QMB_ERR_INVALID, "terms: site out of range");
+            ops[(size_t)i * t->n_col + j] = (uint16_t)(c << 8 | s);
+        }
+        sc[i] = make_double2(t->scalar[2 * i], t->scalar[2 * i + 1]);
+        QMB_REQUIRE(std::isfinite(sc[i].x) && std::isfinite(sc[i].y), QMB_ERR_INVALID,
+                    "terms: non-finite scalar");
+    }
+    h->n_terms = t->n_terms;
+    h->n_col = t->n_col;
+    h->t_nops.alloc(std::max(1, t->n_terms));
+    h->t_ops.alloc(std::max<size_t>(1, ops.size()));
+    h->t_scalar.alloc(std::max(1, t->n_terms));
+    if (t->n_terms) {
+        h->t_nops.upload(nops.data(), nops.size());
+        h->t_ops.upload(ops.data(), ops.size());
+        h->t_scalar.upload(sc.data(), sc.size());
+    }
+}
+
+static size_t gen_smem(const RowGen& rg) {
+    return align16(group_smem_bytes(rg.g)) + terms_smem_bytes(rg.terms);
+}
+
+#define QMB_LOAD_GEN(rg)                                             \
+    extern __shared__ __align__(16) unsigned char smem[];            \
+    GroupSmem gs = load_group((rg).g, smem);                         \
+    TermsSmem ts = load_terms((rg).terms, smem + align16(group_smem_bytes((rg).g)))
+
+// -------------------------------------------------------------- kernels
+__global__ void k_ell_count(RowGen rg, int64_t n, int* __restrict__ cnt) {
+    QMB_LOAD_GEN(rg);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o = rg.orbit_of_row[r];
+        uint64_t src = apply_elem(rg.g, gs, 0, rg.rt.reps[o]);
+        int c = 0;
+        gen_row(rg, gs, ts, src, rg.norms[o], [&](int64_t, double2) { ++c; });
+        cnt[r] = c;
+    }
+}
+
+__global__ void k_slice_width(const int* __restrict__ cnt, int64_t n, int64_t n_slices,
+                              int* __restrict__ width, int64_t* __restrict__ slots) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n_slices;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        int w = 0;
+        for (int i = 0; i < 32; ++i) {
+            int64_t r = s * 32 + i;
+            if (r < n) w = max(w, cnt[r]);
+        }
+        width[s] = w;
+        slots[s] = (int64_t)w * 32;
+    }
+}
+
+template <class M>
+__global__ void k_ell_fill(RowGen rg, int64_t n, const int64_t* __restrict__ off,
+                           const int* __restrict__ width, uint32_t* __restrict__ col,
+                           M* __restrict__ val, M* __restrict__ diag) {
+    QMB_LOAD_GEN(rg);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o = rg.orbit_of_row[r];
+        uint64_t src = apply_elem(rg.g, gs, 0, rg.rt.reps[o]);
+        int64_t s = r >> 5;
+        int64_t base = off[s] + (r & 31);
+        int w = width[s];
+        int j = 0;
+        double2 d = gen_row(rg, gs, ts, src, rg.norms[o], [&](int64_t ot, double2 v) {
+            if (j < w) {
+                col[base + (int64_t)j * 32] = (uint32_t)rg.row_of_orbit[ot];
+                val[base + (int64_t)j * 32] = Sc<M>::from(v);
+            }
+            ++j;
+        });
+        for (; j < w; ++j) {
+            col[base + (int64_t)j * 32] = (uint32_t)r;
+            val[base + (int64_t)j * 32] = Sc<M>::zero();
+        }
+        diag[r] = Sc<M>::from(d);
+    }
+}
+
+// Reference row-major layout over all orbits (null rows: track 0, ind[row*W] = row).
+__global__ void k_ell_ref(RowGen rg, int64_t R, int W, uint32_t* __restrict__ ind,
+                          double2* __restrict__ val, int16_t* __restrict__ track,
+                          int* __restrict__ overflow) {
+    QMB_LOAD_GEN(rg);
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < R;
+         id += (int64_t)gridDim.x * blockDim.x) {
+        ind[id * W] = (uint32_t)id;
+        double ns = rg.norms[id];
+        if (ns < rg.tol) continue;
+        uint64_t src = apply_elem(rg.g, gs, 0, rg.rt.reps[id]);
+        int t = 1;
+        double2 d = gen_row(rg, gs, ts, src, ns, [&](int64_t ot, double2 v) {
+            if (t < W) {
+                ind[id * W + t] = (uint32_t)ot;
+                val[id * W + t] = v;
+            } else {
+                *overflow = 1;
+            }
+            ++t;
+        });
+        val[id * W] = d;
+        track[id] = (int16_t)min(t, 32767);
+    }
+}
+
+template <class Op, class V>
+__global__ void k_hv(Op op, const V* __restrict__ x, V* __restrict__ y) {
+    extern __shared__ __align__(16) unsigned char smem_hv[];
+    op.init(smem_hv);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < op.n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        V xr;
+        y[r] = op.row(r, x, xr);
+    }
+}
+
+template <class M32, class M64>
+__global__ void k_narrow(const M64* __restrict__ a, M32* __restrict__ b, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = cvt<M32>(a[i]);
+}
+
+// ------------------------------------------------------------- helpers
+template <class Op, class V>
+void launch_hv(const Op& op, const V* x, V* y, cudaStream_t st, size_t smem) {
+    const void* fn = (const void*)k_hv<Op, V>;
+    set_group_smem_attr(fn, smem);
+    k_hv<Op, V><<<grid_for(op.n, 256), 256, smem, st>>>(op, x, y);
+    check_launch("k_hv");
+}
+
+void build_sell(qmb_ham_s* h) {
+    RowGen rg = h->row_gen();
+    size_t sm = gen_smem(rg);
+    int64_t n = h->n;
+    DevBuf<int> cnt(n);
+    set_group_smem_attr((const void*)k_ell_count, sm);
+    k_ell_count<<<grid_for(n, 128), 128, sm>>>(rg, n, cnt.p);
+    check_launch("k_ell_count");
+    h->n_slices = (n + 31) / 32;
+    h->slice_w.alloc(h->n_slices);
+    DevBuf<int64_t> slots(h->n_slices + 1);
+    QMB_CUDA_TRY(cudaMemset(slots.p + h->n_slices, 0, sizeof(int64_t)));
+    k_slice_width<<<grid_for(h->n_slices, 256), 256>>>(cnt.p, n, h->n_slices, h->slice_w.p,
+                                                       slots.p);
+    check_launch("k_slice_width");
+    h->slice_off.alloc(h->n_slices + 1);
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, slots.p, h->slice_off.p, h->n_slices + 1);
+    DevBuf<unsigned char> tmp(tb);
+    cub::DeviceScan::ExclusiveSum(tmp.p, tb, slots.p, h->slice_off.p, h->n_slices + 1);
+    QMB_CUDA_TRY(cudaMemcpy(&h->padded, h->slice_off.p + h->n_slices, sizeof(int64_t),
+                            cudaMemcpyDeviceToHost));
+    // statistics
+    std::vector<int> hc(n);
+    cnt.download(hc.data(), n);
+    QMB_CUDA_TRY(cudaDeviceSynchronize());
+    h->nnz = 0;
+    h->max_row = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        h->nnz += hc[i];
+        h->max_row = std::max(h->max_row, hc[i]);
+    }
+    int err = 0;
+    QMB_CUDA_TRY(cudaMemcpy(&err, h->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    QMB_REQUIRE(err == 0, QMB_ERR_INVALID,
+                err == 1 ? "a term changes the number of up spins (not an XXZ-type term)"
+                         : "a target string has no representative (inconsistent group)");
+
+    size_t es = h->cplx ? sizeof(double2) : sizeof(double);
+    h->col.alloc(std::max<int64_t>(h->padded, 1));
+    h->val64.alloc(std::max<int64_t>(h->padded, 1) * es);
+    h->diag64.alloc(n * es);
+    QMB_CUDA_TRY(cudaMemset(h->col.p, 0, sizeof(uint32_t) * h->col.n));
+    QMB_CUDA_TRY(cudaMemset(h->val64.p, 0, h->val64.n));
+    if (h->cplx) {
+        set_group_smem_attr((const void*)k_ell_fill<double2>, sm);
+        k_ell_fill<double2><<<grid_for(n, 128), 128, sm>>>(
+            rg, n, h->slice_off.p, h->slice_w.p, h->col.p, (double2*)h->val64.p,
+            (double2*)h->diag64.p);
+    } else {
+        set_group_smem_attr((const void*)k_ell_fill<double>, sm);
+        k_ell_fill<double><<<grid_for(n, 128), 128, sm>>>(rg, n, h->slice_off.p, h->slice_w.p,
+                                                           h->col.p, (double*)h->val64.p,
+                                                           (double*)h->diag64.p);
+    }
+    check_launch("k_ell_fill");
+    if (h->prec & QMB_PREC_FP32) {
+        size_t e32 = h->cplx ? sizeof(float2) : sizeof(float);
+        h->val32.alloc(std::max<int64_t>(h->padded, 1) * e32);
+        h->diag32.alloc(n * e32);
+        if (h->cplx) {
+            k_narrow<float2, double2><<<grid_for(h->padded, 256), 256>>>(
+                (double2*)h->val64.p, (float2*)h->val32.p, h->padded);
+            k_narrow<float2, double2><<<grid_for(n, 256), 256>>>((double2*)h->diag64.p,
+                                                                (float2*)h->diag32.p, n);
+        } else {
+            k_narrow<float, double><<<grid_for(h->padded, 256), 256>>>(
+                (double*)h->val64.p, (float*)h->val32.p, h->padded);
+            k_narrow<float, double><<<grid_for(n, 256), 256>>>((double*)h->diag64.p,
+                                                              (float*)h->diag32.p, n);
+        }
+        check_launch("k_narrow");
+    }
+    QMB_CUDA_TRY(cudaDeviceSynchronize());
+}
+
+}  // namespace qmb
+
+using namespace qmb;
+
+static bool terms_complex(const qmb_terms* t) {
+    for (int i = 0; i < t->n_terms; ++i)
+        if (std::fabs(t->scalar[2 * i + 1]) > 0.0) return true;
+    return false;
+}
+
+extern "C" qmb_status qmb_ham_create(qmb_sector s, const qmb_terms* terms, int prec,
+                                     qmb_ham* out) {
+    return guarded([&] {
+        QMB_REQUIRE(s && terms && out, QMB_ERR_INVALID, "null argument");
+        *out = nullptr;
+        QMB_REQUIRE(s->has_irrep, QMB_ERR_INVALID, "select an irrep before building H");
+        QMB_REQUIRE((prec & (QMB_PREC_FP64 | QMB_PREC_FP32)) != 0, QMB_ERR_INVALID,
+                    "prec must include QMB_PREC_FP64 and/or QMB_PREC_FP32");
+        QMB_REQUIRE(s->n_active > 0, QMB_ERR_INVALID, "the selected irrep has no active orbit");
+        QMB_REQUIRE(s->n_active < (1ll << 32), QMB_ERR_UNSUPPORTED, "more than 2^32 rows");
+        DeviceGuard dg(s->device);
+        auto h = std::make_unique<qmb_ham_s>();
+        h->sector = s;
+        h->device = s->device;
+        h->n = s->n_active;
+        h->prec = prec | QMB_PREC_FP64;  // FP64 values are always built first
+        h->cplx = !s->is_real || terms_complex(terms);
+        upload_terms(h.get(), terms, s->L);
+        h->err.alloc(1);
+        h->err.zero();
+        build_sell(h.get());
+        if (!(prec & QMB_PREC_FP64)) {
+            // keep FP64 values only when asked for; the matrix-free path needs none
+            h->val64.release();
+            h->prec = prec;
+        }
+        *out = h.release();
+    });
+}
+
+extern "C" qmb_status qmb_ham_destroy(qmb_ham h) {
+    return guarded([&] {
+        if (!h) return;
+        DeviceGuard dg(h->device);
+        delete h;
+    });
+}
+
+extern "C" qmb_status qmb_ham_get_info(qmb_ham h, qmb_ham_info* info) {
+    return guarded([&] {
+        QMB_REQUIRE(h && info, QMB_ERR_INVALID, "null argument");
+        info->n_rows = h->n;
+        info->nnz_offdiag = h->nnz;
+        info->padded = h->padded;
+        info->max_row = h->max_row;
+        info->is_complex = h->cplx ? 1 : 0;
+        info->n_codes = h->n_codes;
+        info->coded = h->coded ? 1 : 0;
+        double vs64 = h->cplx ? 16 : 8, vs32 = h->cplx ? 8 : 4;
+        // compulsory traffic: index + value per off-diagonal, diagonal value,
+        // x read once, y written once
+        info->bytes_fp64 = (double)h->nnz * (4 + vs64) + (double)h->n * (vs64 + 2 * vs64);
+        info->bytes_fp32 = (double)h->nnz * (4 + vs32) + (double)h->n * (vs32 + 2 * vs32);
+    });
+}
+
+extern "C" qmb_status qmb_ham_export_ref(qmb_sector s, const qmb_terms* terms, int W,
+                                         uint32_t* ind, double* val, int16_t* track) {
+    return guarded([&] {
+        QMB_REQUIRE(s && terms && ind && val && track, QMB_ERR_INVALID, "null argument");
+        QMB_REQUIRE(s->has_irrep, QMB_ERR_INVALID, "select an irrep first");
+        QMB_REQUIRE(W >= 1, QMB_ERR_INVALID, "W must be >= 1");
+        DeviceGuard dg(s->device);
+        qmb_ham_s tmp;
+        tmp.sector = s;
+        tmp.device = s->device;
+        upload_terms(&tmp, terms, s->L);
+        tmp.err.alloc(1);
+        tmp.err.zero();
+        RowGen rg = tmp.row_gen();
+        size_t sm = gen_smem(rg);
+        int64_t R = s->R;
+        DevBuf<uint32_t> di((size_t)R * W);
+        DevBuf<double2> dv((size_t)R * W);
+        DevBuf<int16_t> dt(R);
+        DevBuf<int> ov(1);
+        di.zero();
+        dv.zero();
+        dt.zero();
+        ov.zero();
+        set_group_smem_attr((const void*)k_ell_ref, sm);
+        k_ell_ref<<<grid_for(R, 128), 128, sm>>>(rg, R, W, di.p, dv.p, dt.p, ov.p);
+        check_launch("k_ell_ref");
+        int overflow = 0, err = 0;
+        QMB_CUDA_TRY(cudaMemcpy(&overflow, ov.p, sizeof(int), cudaMemcpyDeviceToHost));
+        QMB_CUDA_TRY(cudaMemcpy(&err, tmp.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        QMB_REQUIRE(err == 0, QMB_ERR_INVALID, "a term changes the number of up spins");
+        QMB_REQUIRE(!overflow, QMB_ERR_ELL_OVERFLOW, "a row needs more than W slots");
+        di.download(ind, (size_t)R * W);
+        dv.download(reinterpret_cast<double2*>(val), (size_t)R * W);
+        dt.download(track, R);
+        QMB_CUDA_TRY(cudaDeviceSynchronize());
+    });
+}
+
+extern "C" qmb_status qmb_ham_export_nosym(int L, int n_up, const qmb_terms* terms, int W,
+                                           uint32_t* ind, double* val, int16_t* track,
+                                           int device) {
+    qmb_sector s = nullptr;
+    std::vector<uint32_t> id(L > 0 && L <= 64 ? L : 1);
+    for (int q = 0; q < (int)id.size(); ++q) id[q] = q;
+    qmb_sector_desc d{L, n_up, 1, id.data(), 0, device};
+    qmb_status st = qmb_sector_create(&d, &s);
+    if (st != QMB_OK) return st;
+    double one[2] = {1.0, 0.0};
+    st = qmb_sector_set_irrep(s, one, 0.5);
+    if (st == QMB_OK) st = qmb_ham_export_ref(s, terms, W, ind, val, track);
+    qmb_status st2 = qmb_sector_destroy(s);
+    return st != QMB_OK ? st : st2;
+}
+
+namespace qmb {
+// y = H x dispatch over storage and precision.
+void hv_dispatch(const qmb_ham_s* h, int prec, const void* x, void* y, cudaStream_t st,
+                 bool matrix_free) {
+    bool f64 = (prec == QMB_PREC_FP64);
+    QMB_REQUIRE(prec == QMB_PREC_FP64 || prec == QMB_PREC_FP32, QMB_ERR_INVALID,
+                "prec must be QMB_PREC_FP64 or QMB_PREC_FP32");
+    if (matrix_free) {
+        if (h->cplx) {
+            if (f64) { auto op = h->mf<double2>(); launch_hv(op, (const double2*)x, (double2*)y, st, op.smem_bytes()); }
+            else { auto op = h->mf<float2>(); launch_hv(op, (const float2*)x, (float2*)y, st, op.smem_bytes()); }
+        } else {
+            if (f64) { auto op = h->mf<double>(); launch_hv(op, (const double*)x, (double*)y, st, op.smem_bytes()); }
+            else { auto op = h->mf<float>(); launch_hv(op, (const float*)x, (float*)y, st, op.smem_bytes()); }
+        }
+        return;
+    }
+    QMB_REQUIRE(f64 ? h->val64.p != nullptr : h->val32.p != nullptr, QMB_ERR_INVALID,
+                "the handle does not hold values of the requested precision");
+    if (h->cplx) {
+        if (f64) launch_hv(h->sell<double2>(true), (const double2*)x, (double2*)y, st, 0);
+        else launch_hv(h->sell<float2>(false), (const float2*)x, (float2*)y, st, 0);
+    } else {
+        if (f64) launch_hv(h->sell<double>(true), (const double*)x, (double*)y, st, 0);
+        else launch_hv(h->sell<float>(false), (const float*)x, (float*)y, st, 0);
+    }
+}
+}  // namespace qmb
+
+extern "C" qmb_status qmb_hv(qmb_ham h, int prec, const void* x_dev, void* y_dev, void* stream) {
+    return guarded([&] {
+        QMB_REQUIRE(h && x_dev && y_dev, QMB_ERR_INVALID, "null argument");
+        DeviceGuard dg(h->device);
+        hv_dispatch(h, prec, x_dev, y_dev, (cudaStream_t)stream, false);
+    });
+}
+
+extern "C" qmb_status qmb_hv_matrix_free(qmb_ham h, int prec, const void* x_dev, void* y_dev,
+                                         void* stream) {
+    return guarded([&] {
+        QMB_REQUIRE(h && x_dev && y_dev, QMB_ERR_INVALID, "null argument");
+        DeviceGuard dg(h->device);
+        hv_dispatch(h, prec, x_dev, y_dev, (cudaStream_t)stream, true);
+    });
+}
+
+extern "C" qmb_status qmb_hv_host(qmb_ham h, int prec, const void* x, void* y) {
+    return guarded([&] {
+        QMB_REQUIRE(h && x && y, QMB_ERR_INVALID, "null argument");
+        DeviceGuard dg(h->device);
+        size_t es = (prec == QMB_PREC_FP64 ? 8 : 4) * (h->cplx ? 2 : 1);
+        DevBuf<unsigned char> dx(h->n * es), dy(h->n * es);
+        QMB_CUDA_TRY(cudaMemcpy(dx.p, x, h->n * es, cudaMemcpyHostToDevice));
+        hv_dispatch(h, prec, dx.p, dy.p, 0, false);
+        QMB_CUDA_TRY(cudaMemcpy(y, dy.p, h->n * es, cudaMemcpyDeviceToHost));
+    });
+}

@@ -1,0 +1,718 @@
+// qmb_lanczos.cu -- ground-state Lanczos on one GPU.
+//
+// Replaces LanczosEigVals_CUDA / LanczosEigenStateFromSeed
+// (exact_diagonalization/lanczos.cu:31-317).  The reference runs ~14 vector
+// passes per step through thrust and cuBLAS (a handle created and destroyed
+// per call, host-synchronising scalars).  Here one step is two kernels:
+//   K1  y = H (w_j / beta_j) - beta_j v_{j-1};  v_j = w_j / beta_j;  alpha_j = <v_j, y>
+//   K2  w_{j+1} = y - alpha_j v_j;  beta_{j+1} = ||w_{j+1}||
+// with FP64 scalars kept on the device (deterministic last-block reductions)
+// and the step index read from device memory, so a step is a replayable CUDA
+// graph.  Optional full reorthogonalisation runs classical Gram-Schmidt
+// passes against the stored Krylov basis.  The tridiagonal eigenproblem is
+// solved on the host in FP64 every `check_every` steps.
+#include <curand_kernel.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "qmb_ham.cuh"
+#include "qmb_lanczos.cuh"
+#include "qmb_tridiag.h"
+
+namespace qmb {
+
+constexpr int kLzBlock = 256;
+
+struct LzDev {
+    double* alpha;      // [cap]
+    double* beta;       // [cap + 1]
+    int* iter;
+    unsigned* counter;
+    double* partials;   // [2 * max_blocks]
+    double2* coefs;     // [cap + 1]
+    double* cpart;      // [2 * max_blocks * (cap + 1)]
+    double* scratch;    // [4]
+};
+
+__host__ __device__ inline uint64_t splitmix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double splitmix_uniform(uint64_t seed, uint64_t i) {
+    uint64_t z = splitmix64(seed + i);
+    return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// ----------------------------------------------------------------- kernels
+// Start vector w_0 (unnormalised) and beta_0 = ||w_0||; resets the step.
+// mode 0: uniform(-1,1) from splitmix64(seed + i) (complex: seed + 2i, 2i+1)
+// mode 1: curand_init(seed + i, 0, 0) then curand_uniform (complex: two draws),
+//         the start vector of init_random_vec (utils/misc_funcs_gpu.cu:31-52)
+// mode 2: copy of `from`
+template <class V, class P>
+__global__ void k_lz_start(int64_t n, int mode, uint64_t seed, const P* __restrict__ from,
+                           V* __restrict__ w0, LzDev d) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        V v;
+        if (mode == 2) {
+            v = cvt<V>(from[i]);
+        } else if (mode == 1) {
+            curandState st;
+            curand_init((unsigned long long)(seed + (uint64_t)i), 0ull, 0ull, &st);
+            float a = curand_uniform(&st);
+            if constexpr (Sc<V>::cplx) {
+                float b = curand_uniform(&st);
+                v = Sc<V>::from(make_double2(a, b));
+            } else {
+                v = Sc<V>::from(make_double2(a, 0.0));
+            }
+        } else {
+            if constexpr (Sc<V>::cplx)
+                v = Sc<V>::from(make_double2(splitmix_uniform(seed, 2 * i), splitmix_uniform(seed, 2 * i + 1)));
+            else
+                v = Sc<V>::from(make_double2(splitmix_uniform(seed, i), 0.0));
+        }
+        w0[i] = v;
+        acc += Sc<V>::abs2(v);
+    }
+    double tot;
+    if (grid_reduce(acc, d.partials, d.counter, red, &tot) && threadIdx.x == 0) {
+        d.beta[0] = sqrt(tot);
+        *d.iter = 0;
+    }
+}
+
+// K1: y = H w_j / beta_j - beta_j v_{j-1}; v_j = w_j / beta_j; alpha_j = Re <v_j, y>.
+// Optionally psi += c_j v_j (eigenvector regeneration).
+template <class Op, class V, class P>
+__global__ void __launch_bounds__(kLzBlock) k_lz_hv(Op op, V* __restrict__ wbuf, V* __restrict__ vring,
+                                                    int K, LzDev d, const double* __restrict__ ritz,
+                                                    P* __restrict__ psi) {
+    extern __shared__ __align__(16) unsigned char smem_lz[];
+    __shared__ double red[32];
+    op.init(smem_lz);
+    const int64_t n = op.n;
+    const int j = *d.iter;
+    const V* X = wbuf + (int64_t)(j & 1) * n;
+    V* Y = wbuf + (int64_t)((j + 1) & 1) * n;
+    V* Vc = vring + (int64_t)(j % K) * n;
+    const V* Vp = vring + (int64_t)((j + K - 1) % K) * n;
+    const double bj = d.beta[j];
+    const double inv = 1.0 / bj;
+    const double c = ritz ? ritz[j] : 0.0;
+    double acc = 0.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        V xr;
+        V hx = op.row(r, X, xr);
+        V vj = Sc<V>::scale(xr, inv);
+        V y = Sc<V>::scale(hx, inv);
+        if (j > 0) y = Sc<V>::sub(y, Sc<V>::scale(Vp[r], bj));
+        Vc[r] = vj;
+        Y[r] = y;
+        acc += Sc<V>::re_conj_mul(vj, y);
+        if (psi) psi[r] = Sc<P>::add(psi[r], Sc<P>::scale(cvt<P>(vj), c));
+    }
+    double tot;
+    if (grid_reduce(acc, d.partials, d.counter, red, &tot) && threadIdx.x == 0) d.alpha[j] = tot;
+}
+
+// K2: w_{j+1} = y - alpha_j v_j; beta_{j+1} = ||w_{j+1}||; finalize advances the step.
+template <class V>
+__global__ void __launch_bounds__(kLzBlock) k_lz_update(int64_t n, V* __restrict__ wbuf,
+                                                        const V* __restrict__ vring, int K,
+                                                        LzDev d, int finalize) {
+    __shared__ double red[32];
+    const int j = *d.iter;
+    V* Y = wbuf + (int64_t)((j + 1) & 1) * n;
+    const V* Vc = vring + (int64_t)(j % K) * n;
+    const double a = d.alpha[j];
+    double acc = 0.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        V y = Sc<V>::sub(Y[r], Sc<V>::scale(Vc[r], a));
+        Y[r] = y;
+        acc += Sc<V>::abs2(y);
+    }
+    double tot;
+    if (grid_reduce(acc, d.partials, d.counter, red, &tot) && threadIdx.x == 0) {
+        d.beta[j + 1] = sqrt(tot);
+        if (finalize) *d.iter = j + 1;
+    }
+}
+
+// Reorthogonalisation, pass 1: coefs[i] = <v_i, w_{j+1}> for i <= j.
+template <class V>
+__global__ void __launch_bounds__(kLzBlock) k_reorth_dots(int64_t n, const V* __restrict__ wbuf,
+                                                          const V* __restrict__ vring, LzDev d) {
+    __shared__ double red[32];
+    __shared__ bool last;
+    const int j = *d.iter;
+    const V* Y = wbuf + (int64_t)((j + 1) & 1) * n;
+    const int nb = gridDim.x;
+    for (int i = 0; i <= j; ++i) {
+        const V* Vi = vring + (int64_t)i * n;
+        double re = 0.0, im = 0.0;
+        for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+             r += (int64_t)gridDim.x * blockDim.x) {
+            V v = Vi[r], y = Y[r];
+            re += Sc<V>::re_conj_mul(v, y);
+            if constexpr (Sc<V>::cplx) im += Sc<V>::im_conj_mul(v, y);
+        }
+        double bre = block_sum(re, red);
+        double bim = Sc<V>::cplx ? block_sum(im, red) : 0.0;
+        if (threadIdx.x == 0) {
+            d.cpart[2 * ((int64_t)i * nb + blockIdx.x)] = bre;
+            d.cpart[2 * ((int64_t)i * nb + blockIdx.x) + 1] = bim;
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned t = atomicAdd(d.counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int b = 0; b < nb; ++b) {
+            re += __ldcg(d.cpart + 2 * ((int64_t)i * nb + b));
+            im += __ldcg(d.cpart + 2 * ((int64_t)i * nb + b) + 1);
+        }
+        d.coefs[i] = make_double2(re, im);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *d.counter = 0;
+}
+
+// Reorthogonalisation, pass 2: w_{j+1} -= sum_i coefs[i] v_i; beta_{j+1} = ||w_{j+1}||.
+template <class V>
+__global__ void __launch_bounds__(kLzBlock) k_reorth_update(int64_t n, V* __restrict__ wbuf,
+                                                            const V* __restrict__ vring, LzDev d,
+                                                            int finalize) {
+    extern __shared__ __align__(16) unsigned char smem_ro[];
+    __shared__ double red[32];
+    double2* cf = reinterpret_cast<double2*>(smem_ro);
+    const int j = *d.iter;
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) cf[i] = d.coefs[i];
+    __syncthreads();
+    V* Y = wbuf + (int64_t)((j + 1) & 1) * n;
+    double acc = 0.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        V y = Y[r];
+        for (int i = 0; i <= j; ++i) {
+            V v = vring[(int64_t)i * n + r];
+            y = Sc<V>::sub(y, Sc<V>::mul(Sc<V>::from(cf[i]), v));
+        }
+        Y[r] = y;
+        acc += Sc<V>::abs2(y);
+    }
+    double tot;
+    if (grid_reduce(acc, d.partials, d.counter, red, &tot) && threadIdx.x == 0) {
+        d.beta[j + 1] = sqrt(tot);
+        if (finalize) *d.iter = j + 1;
+    }
+}
+
+// psi = sum_i ritz[i] v_i over a stored basis.
+template <class V, class P>
+__global__ void k_ritz(int64_t n, const V* __restrict__ vring, int m,
+                       const double* __restrict__ ritz, P* __restrict__ psi) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        P acc = Sc<P>::zero();
+        for (int i = 0; i < m; ++i)
+            acc = Sc<P>::add(acc, Sc<P>::scale(cvt<P>(vring[(int64_t)i * n + r]), ritz[i]));
+        psi[r] = acc;
+    }
+}
+
+// scratch[0] = ||H psi - theta psi||^2, scratch[1] = ||psi||^2.
+template <class Op, class P>
+__global__ void k_residual(Op op, const P* __restrict__ psi, double theta, LzDev d) {
+    extern __shared__ __align__(16) unsigned char smem_rs[];
+    __shared__ double red[32];
+    op.init(smem_rs);
+    double a = 0.0, b = 0.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < op.n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        P xr;
+        P hx = op.row(r, psi, xr);
+        P res = Sc<P>::sub(hx, Sc<P>::scale(xr, theta));
+        a += Sc<P>::abs2(res);
+        b += Sc<P>::abs2(xr);
+    }
+    double ta, tb;
+    bool la = grid_reduce(a, d.partials, d.counter, red, &ta);
+    if (la && threadIdx.x == 0) d.scratch[0] = ta;
+    __syncthreads();
+    bool lb = grid_reduce(b, d.partials + gridDim.x, d.counter + 1, red, &tb);
+    if (lb && threadIdx.x == 0) d.scratch[1] = tb;
+}
+
+// ------------------------------------------------------------------- host
+int lz_blocks() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 4;
+}
+
+struct LzState {
+    int cap = 0;
+    int nb = 0;
+    DevBuf<double> alpha, beta, partials, cpart, scratch;
+    DevBuf<int> iter;
+    DevBuf<unsigned> counter;
+    DevBuf<double2> coefs;
+    LzDev d{};
+    void init(int cap_, int nb_, bool reorth) {
+        cap = cap_;
+        nb = nb_;
+        alpha.alloc(cap + 1);
+        beta.alloc(cap + 2);
+        partials.alloc(2 * (size_t)nb);
+        scratch.alloc(4);
+        iter.alloc(1);
+        counter.alloc(2);
+        counter.zero();
+        iter.zero();
+        coefs.alloc(reorth ? cap + 2 : 1);
+        cpart.alloc(reorth ? 2 * (size_t)nb * (cap + 2) : 1);
+        d.alpha = alpha.p;
+        d.beta = beta.p;
+        d.iter = iter.p;
+        d.counter = counter.p;
+        d.partials = partials.p;
+        d.coefs = coefs.p;
+        d.cpart = cpart.p;
+        d.scratch = scratch.p;
+    }
+};
+
+struct PhaseOut {
+    int m = 0;            // Lanczos vectors used (tridiagonal size)
+    double theta = 0.0;
+    double est = 0.0;     // residual estimate beta_m |s_{m-1}|
+    bool converged = false;
+    std::vector<double> a, e, s;
+    int n_hv = 0;
+};
+
+struct PhaseOpts {
+    int max_iter = 200;
+    int min_iter = 1;
+    double tol = 1e-12;       // <= 0: run exactly max_iter steps
+    double stall_tol = 0.0;   // stop when |d theta| < stall_tol*|theta| between checks
+    int reorth = 0;           // CGS passes
+    int check_every = 10;
+    bool use_graph = true;
+};
+
+// Runs one Lanczos phase for operator op with vectors of type V.
+// start_mode 0/1: generated from seed, 2: copied from `from` (type P).
+template <class Op, class V, class P>
+PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_mode,
+                   uint64_t seed, const P* from, bool store, DevBuf<V>& vring, int& K,
+                   DevBuf<V>& wbuf, LzState& st, cudaStream_t s) {
+    const int64_t n = op.n;
+    PhaseOut out;
+    int cap = std::max(1, (int)std::min<int64_t>(po.max_iter, n));
+    K = store ? cap + 1 : 2;
+    vring.alloc((size_t)K * n);
+    wbuf.alloc(2 * (size_t)n);
+    st.init(cap, lz_blocks(), po.reorth > 0);
+    const int nb = st.nb;
+    QMB_REQUIRE(po.reorth == 0 || store, QMB_ERR_INVALID, "reorthogonalisation needs the stored basis");
+
+    k_lz_start<V, P><<<nb, kLzBlock, 0, s>>>(n, start_mode, seed, from, wbuf.p, st.d);
+    check_launch("k_lz_start");
+
+    const void* f1 = (const void*)k_lz_hv<Op, V, P>;
+    set_group_smem_attr(f1, op_smem);
+    size_t ro_smem = sizeof(double2) * (size_t)(cap + 2);
+    if (po.reorth) set_group_smem_attr((const void*)k_reorth_update<V>, ro_smem);
+
+    auto step = [&](cudaStream_t ss) {
+        k_lz_hv<Op, V, P><<<nb, kLzBlock, op_smem, ss>>>(op, wbuf.p, vring.p, K, st.d, nullptr,
+                                                         (P*)nullptr);
+        k_lz_update<V><<<nb, kLzBlock, 0, ss>>>(n, wbuf.p, vring.p, K, st.d, po.reorth ? 0 : 1);
+        for (int p = 0; p < po.reorth; ++p) {
+            k_reorth_dots<V><<<nb, kLzBlock, 0, ss>>>(n, wbuf.p, vring.p, st.d);
+            k_reorth_update<V><<<nb, kLzBlock, ro_smem, ss>>>(n, wbuf.p, vring.p, st.d,
+                                                              p == po.reorth - 1 ? 1 : 0);
+        }
+    };
+
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    if (po.use_graph) {
+        QMB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        step(s);
+        cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            exec = nullptr;
+        }
+    }
+    check_launch("lanczos step capture");
+
+    std::vector<double> ha(cap + 1), hb(cap + 2);
+    int done = 0;
+    double theta_prev = 0.0;
+    bool have_prev = false;
+    const int every = std::max(1, po.check_every);
+    while (done < cap) {
+        int todo = std::min(every, cap - done);
+        for (int t = 0; t < todo; ++t) {
+            if (exec) QMB_CUDA_TRY(cudaGraphLaunch(exec, s));
+            else step(s);
+        }
+        check_launch("lanczos step");
+        done += todo;
+        out.n_hv += todo;
+        QMB_CUDA_TRY(cudaMemcpyAsync(ha.data(), st.alpha.p, sizeof(double) * done,
+                                     cudaMemcpyDeviceToHost, s));
+        QMB_CUDA_TRY(cudaMemcpyAsync(hb.data(), st.beta.p, sizeof(double) * (done + 1),
+                                     cudaMemcpyDeviceToHost, s));
+        QMB_CUDA_TRY(cudaStreamSynchronize(s));
+        // a (near) zero beta ends the Krylov space: keep the steps up to it
+        bool breakdown = false;
+        for (int i = done - todo; i < done; ++i) {
+            double sc_i = std::fabs(ha[i]) + (i > 0 ? std::fabs(hb[i]) : 0.0) + 1e-300;
+            if (!(hb[i + 1] > 1e-13 * sc_i)) {
+                QMB_REQUIRE(std::isfinite(ha[i]), QMB_ERR_INVALID,
+                            "non-finite Lanczos coefficient (check the Hamiltonian)");
+                done = i + 1;
+                breakdown = true;
+                break;
+            }
+            QMB_REQUIRE(std::isfinite(ha[i]) && std::isfinite(hb[i + 1]), QMB_ERR_INVALID,
+                        "non-finite Lanczos coefficient (check the Hamiltonian)");
+        }
+        // tridiagonal of the first `done` steps
+        double theta = tridiag_min_eig(ha.data(), hb.data() + 1, done);
+        std::vector<double> sv(done);
+        tridiag_eigvec(ha.data(), hb.data() + 1, done, theta, sv.data());
+        double est = hb[done] * std::fabs(sv[done - 1]);
+        double scale = std::max(std::fabs(theta), 1e-300);
+        if (breakdown) est = 0.0;
+        out.m = done;
+        out.theta = theta;
+        out.est = est;
+        out.s = sv;
+        if (breakdown) {
+            out.converged = true;
+            break;
+        }
+        if (po.tol > 0 && done >= po.min_iter) {
+            bool res_ok = est <= po.tol * scale;
+            bool dth_ok = have_prev && std::fabs(theta - theta_prev) <= po.tol * scale;
+            bool stall = po.stall_tol > 0 && have_prev &&
+                         std::fabs(theta - theta_prev) <= po.stall_tol * scale;
+            if ((res_ok && dth_ok) || stall) {
+                out.converged = res_ok && dth_ok;
+                break;
+            }
+        }
+        theta_prev = theta;
+        have_prev = true;
+    }
+    if (po.tol <= 0) out.converged = true;
+    out.a.assign(ha.begin(), ha.begin() + out.m);
+    out.e.assign(hb.begin() + 1, hb.begin() + out.m);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    return out;
+}
+
+// psi = Ritz vector of a finished phase (stored basis, else regeneration).
+template <class Op, class V, class P>
+void ritz_vector(const Op& op, size_t op_smem, const PhaseOut& ph, int start_mode, uint64_t seed,
+                 const P* from, bool stored, DevBuf<V>& vring, int K, DevBuf<V>& wbuf,
+                 LzState& st, P* psi, int& n_hv, cudaStream_t s) {
+    const int64_t n = op.n;
+    DevBuf<double> ritz(ph.m);
+    ritz.upload(ph.s.data(), ph.m, s);
+    if (stored) {
+        k_ritz<V, P><<<grid_for(n, 256), 256, 0, s>>>(n, vring.p, ph.m, ritz.p, psi);
+        check_launch("k_ritz");
+        QMB_CUDA_TRY(cudaStreamSynchronize(s));
+        return;
+    }
+    // regenerate v_0..v_{m-1} with the same start; kernels are deterministic
+    QMB_CUDA_TRY(cudaMemsetAsync(psi, 0, sizeof(P) * n, s));
+    const int nb = st.nb;
+    k_lz_start<V, P><<<nb, kLzBlock, 0, s>>>(n, start_mode, seed, from, wbuf.p, st.d);
+    for (int j = 0; j < ph.m; ++j) {
+        k_lz_hv<Op, V, P><<<nb, kLzBlock, op_smem, s>>>(op, wbuf.p, vring.p, K, st.d, ritz.p, psi);
+        if (j + 1 < ph.m) k_lz_update<V><<<nb, kLzBlock, 0, s>>>(n, wbuf.p, vring.p, K, st.d, 1);
+        ++n_hv;
+    }
+    check_launch("regenerate");
+    QMB_CUDA_TRY(cudaStreamSynchronize(s));
+}
+
+template <class Op, class P>
+double residual_norm(const Op& op, size_t op_smem, const P* psi, double theta, LzState& st,
+                     cudaStream_t s, double* psi_norm2) {
+    set_group_smem_attr((const void*)k_residual<Op, P>, op_smem);
+    k_residual<Op, P><<<st.nb, kLzBlock, op_smem, s>>>(op, psi, theta, st.d);
+    check_launch("k_residual");
+    double h[2];
+    QMB_CUDA_TRY(cudaMemcpyAsync(h, st.scratch.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    QMB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (psi_norm2) *psi_norm2 = h[1];
+    return std::sqrt(h[0] / std::max(h[1], 1e-300));
+}
+
+bool fits_device(size_t bytes) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+    return bytes < fr * 0.6;
+}
+
+// Full solve for one storage / precision combination.
+//   V32/V64: vector types of the low / high phase, Op32/Op64 the operators.
+template <class Op32, class Op64, class V32, class V64>
+void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t sm64,
+           const qmb_lanczos_opts& o, qmb_lanczos_result* res, double* coeffs, int64_t n_coeffs) {
+    cudaStream_t s;
+    QMB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct SG { cudaStream_t s; ~SG() { cudaStreamDestroy(s); } } sg{s};
+    cudaEvent_t e0, e1;
+    QMB_CUDA_TRY(cudaEventCreate(&e0));
+    QMB_CUDA_TRY(cudaEventCreate(&e1));
+    struct EG { cudaEvent_t a, b; ~EG() { cudaEventDestroy(a); cudaEventDestroy(b); } } eg{e0, e1};
+    QMB_CUDA_TRY(cudaEventRecord(e0, s));
+    const int64_t n = h->n;
+    std::memset(res, 0, sizeof(*res));
+    res->ms_hv = -1;
+    LzState st;
+    PhaseOpts po;
+    po.max_iter = o.max_iter;
+    po.min_iter = std::max(1, o.min_iter);
+    po.tol = o.tol;
+    po.reorth = o.reorth;
+    po.check_every = o.check_every > 0 ? o.check_every : 10;
+    const int cap = std::max(1, (int)std::min<int64_t>(o.max_iter, n));
+    int n_hv = 0;
+    DevBuf<V64> psi(n);
+    double theta = 0.0;
+    int iters = 0;
+    bool conv = false;
+    PhaseOut last;
+
+    if (o.mode == QMB_MODE_FP64) {
+        bool store = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap + 3) * n);
+        QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
+        DevBuf<V64> vr, wb;
+        int K;
+        last = run_phase<Op64, V64, V64>(op64, sm64, po, o.start, o.seed, nullptr, store, vr, K, wb, st, s);
+        n_hv += last.n_hv;
+        ritz_vector<Op64, V64, V64>(op64, sm64, last, o.start, o.seed, nullptr, store, vr, K, wb, st,
+                                    psi.p, n_hv, s);
+        theta = last.theta;
+        iters = last.m;
+        conv = last.converged;
+    } else {
+        // low phase: FP32 vectors and values, FP64 scalars
+        PhaseOpts p1 = po;
+        if (o.mode == QMB_MODE_MIXED) {
+            p1.tol = std::max(o.tol, 1e-6);
+            p1.stall_tol = 2e-7;
+        }
+        bool store = o.reorth > 0 || fits_device(sizeof(V32) * (size_t)(cap + 3) * n);
+        QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
+        PhaseOut ph1;
+        {
+            DevBuf<V32> vr, wb;
+            int K;
+            ph1 = run_phase<Op32, V32, V64>(op32, sm32, p1, o.start, o.seed, nullptr, store, vr, K, wb, st, s);
+            n_hv += ph1.n_hv;
+            ritz_vector<Op32, V32, V64>(op32, sm32, ph1, o.start, o.seed, nullptr, store, vr, K, wb,
+                                        st, psi.p, n_hv, s);
+        }
+        res->E0_low = ph1.theta;
+        res->iters_low = ph1.m;
+        theta = ph1.theta;
+        iters = ph1.m;
+        conv = ph1.converged;
+        last = ph1;
+        if (o.mode == QMB_MODE_MIXED) {
+            // FP64 restart from the FP32 Ritz vector
+            PhaseOpts p2 = po;
+            p2.max_iter = o.refine_max_iter > 0 ? o.refine_max_iter : 60;
+            p2.min_iter = 2;
+            p2.check_every = std::min(po.check_every, 5);
+            int cap2 = std::max(1, (int)std::min<int64_t>(p2.max_iter, n));
+            bool store2 = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap2 + 3) * n);
+            DevBuf<V64> start(n);
+            QMB_CUDA_TRY(cudaMemcpyAsync(start.p, psi.p, sizeof(V64) * n, cudaMemcpyDeviceToDevice, s));
+            DevBuf<V64> vr, wb;
+            int K;
+            PhaseOut ph2 = run_phase<Op64, V64, V64>(op64, sm64, p2, 2, 0, start.p, store2, vr, K,
+                                                     wb, st, s);
+            n_hv += ph2.n_hv;
+            ritz_vector<Op64, V64, V64>(op64, sm64, ph2, 2, 0, start.p, store2, vr, K, wb, st,
+                                        psi.p, n_hv, s);
+            theta = ph2.theta;
+            iters += ph2.m;
+            conv = ph2.converged;
+            last = ph2;
+        }
+    }
+    double pn2 = 0;
+    res->residual = residual_norm<Op64, V64>(op64, sm64, psi.p, theta, st, s, &pn2);
+    ++n_hv;
+    res->residual_ref = res->residual * std::sqrt(pn2) / (double)n;
+    QMB_CUDA_TRY(cudaEventRecord(e1, s));
+    QMB_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    res->ms_total = ms;
+    res->E0 = theta;
+    res->iters = iters;
+    res->n_hv = n_hv;
+    res->converged = conv ? 1 : 0;
+    if (o.mode == QMB_MODE_FP64) res->E0_low = theta;
+    if (coeffs) {
+        for (int64_t i = 0; i < n_coeffs; ++i) coeffs[i] = i < (int64_t)last.s.size() ? last.s[i] : 0.0;
+    }
+    if (o.want_vector) {
+        h->psi.alloc(sizeof(V64) * n);
+        QMB_CUDA_TRY(cudaMemcpy(h->psi.p, psi.p, sizeof(V64) * n, cudaMemcpyDeviceToDevice));
+        h->psi_n = n;
+    }
+}
+
+}  // namespace qmb
+
+using namespace qmb;
+
+extern "C" void qmb_lanczos_default_opts(qmb_lanczos_opts* o) {
+    if (!o) return;
+    o->mode = QMB_MODE_FP64;
+    o->max_iter = 300;
+    o->min_iter = 5;
+    o->tol = 1e-12;
+    o->reorth = 0;
+    o->start = QMB_START_SPLITMIX;
+    o->seed = 20261203ull;
+    o->check_every = 10;
+    o->hv = QMB_HV_STORED;
+    o->refine_max_iter = 60;
+    o->want_vector = 0;
+}
+
+extern "C" qmb_status qmb_lanczos(qmb_ham h, const qmb_lanczos_opts* opts, qmb_lanczos_result* res,
+                                  double* krylov_coeffs, int64_t n_coeffs) {
+    return guarded([&] {
+        QMB_REQUIRE(h && opts && res, QMB_ERR_INVALID, "null argument");
+        const qmb_lanczos_opts& o = *opts;
+        QMB_REQUIRE(o.mode >= 0 && o.mode <= 2, QMB_ERR_INVALID, "unknown mode");
+        QMB_REQUIRE(o.max_iter >= 1 && o.max_iter <= 4096, QMB_ERR_INVALID, "max_iter must be in 1..4096");
+        QMB_REQUIRE(o.reorth >= 0 && o.reorth <= 2, QMB_ERR_INVALID, "reorth must be 0, 1 or 2");
+        QMB_REQUIRE(o.start == QMB_START_SPLITMIX || o.start == QMB_START_CURAND, QMB_ERR_INVALID,
+                    "unknown start-vector mode");
+        QMB_REQUIRE(o.hv == QMB_HV_STORED || o.hv == QMB_HV_MATRIX_FREE, QMB_ERR_INVALID, "unknown hv");
+        DeviceGuard dg(h->device);
+        bool mf = o.hv == QMB_HV_MATRIX_FREE;
+        bool need64 = o.mode != QMB_MODE_FP32;
+        bool need32 = o.mode != QMB_MODE_FP64;
+        if (!mf) {
+            QMB_REQUIRE(!need64 || h->val64.p, QMB_ERR_INVALID, "handle holds no FP64 values");
+            QMB_REQUIRE(!need32 || h->val32.p, QMB_ERR_INVALID, "handle holds no FP32 values");
+        }
+        if (h->cplx) {
+            if (mf) {
+                auto a = h->mf<float2>();
+                auto b = h->mf<double2>();
+                solve<MfOp<float2>, MfOp<double2>, float2, double2>(h, a, a.smem_bytes(), b, b.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
+            } else if (!need32) {
+                auto b = h->sell<double2>(true);
+                solve<SellOp<double2>, SellOp<double2>, float2, double2>(h, b, 0, b, 0, o, res, krylov_coeffs, n_coeffs);
+            } else if (!need64) {
+                auto a = h->sell<float2>(false);
+                solve<SellOp<float2>, SellOp<float2>, float2, double2>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
+            } else {
+                solve<SellOp<float2>, SellOp<double2>, float2, double2>(h, h->sell<float2>(false), 0, h->sell<double2>(true), 0, o, res, krylov_coeffs, n_coeffs);
+            }
+        } else {
+            if (mf) {
+                auto a = h->mf<float>();
+                auto b = h->mf<double>();
+                solve<MfOp<float>, MfOp<double>, float, double>(h, a, a.smem_bytes(), b, b.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
+            } else if (!need32) {
+                auto b = h->sell<double>(true);
+                solve<SellOp<double>, SellOp<double>, float, double>(h, b, 0, b, 0, o, res, krylov_coeffs, n_coeffs);
+            } else if (!need64) {
+                auto a = h->sell<float>(false);
+                solve<SellOp<float>, SellOp<float>, float, double>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
+            } else {
+                solve<SellOp<float>, SellOp<double>, float, double>(h, h->sell<float>(false), 0, h->sell<double>(true), 0, o, res, krylov_coeffs, n_coeffs);
+            }
+        }
+        if (!res->converged && o.tol > 0) throw Error{QMB_ERR_NOT_CONVERGED, "Lanczos did not reach the tolerance within max_iter"};
+    });
+}
+
+extern "C" qmb_status qmb_ground_state(qmb_ham h, void* psi, int64_t n) {
+    return guarded([&] {
+        QMB_REQUIRE(h && psi, QMB_ERR_INVALID, "null argument");
+        QMB_REQUIRE(h->psi.p && h->psi_n == n, QMB_ERR_INVALID,
+                    "no ground state kept (run qmb_lanczos with want_vector) or wrong length");
+        DeviceGuard dg(h->device);
+        QMB_CUDA_TRY(cudaMemcpy(psi, h->psi.p, h->psi.n, cudaMemcpyDeviceToHost));
+    });
+}
+
+extern "C" qmb_status qmb_lanczos_ref_ell(float* E, int n_iter, int nobv, int max_terms,
+                                          long long seed, const uint32_t* ind_dev,
+                                          const void* val_dev, const int16_t* track_dev,
+                                          int is_complex, float* krylov_out, int check_eig_state,
+                                          float* residual) {
+    return guarded([&] {
+        QMB_REQUIRE(E && ind_dev && val_dev && track_dev, QMB_ERR_INVALID, "null argument");
+        QMB_REQUIRE(nobv >= 1 && max_terms >= 1 && n_iter >= 1 && n_iter <= 4096, QMB_ERR_INVALID,
+                    "bad sizes");
+        int dev = 0;
+        QMB_CUDA_TRY(cudaGetDevice(&dev));
+        qmb_ham_s dummy;
+        dummy.n = nobv;
+        qmb_lanczos_opts o;
+        qmb_lanczos_default_opts(&o);
+        o.mode = QMB_MODE_FP32;
+        o.max_iter = std::min(n_iter, nobv);
+        o.tol = 0.0;
+        o.start = QMB_START_CURAND;
+        o.seed = (uint64_t)seed;
+        o.check_every = o.max_iter;
+        qmb_lanczos_result r;
+        std::vector<double> cf(o.max_iter);
+        if (is_complex) {
+            RefEllOp<float2> op{nobv, max_terms, ind_dev, (const float2*)val_dev, track_dev};
+            solve<RefEllOp<float2>, RefEllOp<float2>, float2, double2>(&dummy, op, 0, op, 0, o, &r, cf.data(), o.max_iter);
+        } else {
+            RefEllOp<float> op{nobv, max_terms, ind_dev, (const float*)val_dev, track_dev};
+            solve<RefEllOp<float>, RefEllOp<float>, float, double>(&dummy, op, 0, op, 0, o, &r, cf.data(), o.max_iter);
+        }
+        *E = (float)r.E0;
+        if (krylov_out)
+            for (int i = 0; i < n_iter; ++i) krylov_out[i] = i < o.max_iter ? (float)cf[i] : 0.0f;
+        if (residual) *residual = check_eig_state ? (float)r.residual_ref : 0.0f;
+    });
+}

@@ -1,0 +1,56 @@
+// qmb_sector.cuh -- internal sector object shared by the modules.
+#pragma once
+#include <complex>
+#include <vector>
+
+#include "qmb_group.cuh"
+
+struct qmb_sector_s {
+    int device = 0;
+    int L = 0, n_up = 0, G = 0, n_ext = 0, flip = 0;
+    int64_t n_states = 0, R = 0, n_active = 0;
+    std::vector<uint32_t> perm;  // host copy [G][L]
+
+    // group on device
+    int structured = 0, W = 0, n_chunks = 0;
+    qmb::DevBuf<qmb::ElemRot> rot;
+    qmb::DevBuf<uint64_t> tables;
+
+    // orbit table
+    qmb::DevBuf<uint64_t> reps;     // [R] ascending
+    qmb::DevBuf<uint32_t> bucket;   // [2^T + 1]
+    int T = 0;
+
+    // selected irrep
+    bool has_irrep = false;
+    bool is_real = true;
+    double tol_norm = 1e-5;
+    std::vector<std::complex<double>> chars;  // [n_ext]
+    qmb::DevBuf<double2> chars_dev;           // [n_ext]
+    qmb::DevBuf<double> norms;                // [R]
+    qmb::DevBuf<int64_t> row_of_orbit;        // [R], -1 for null orbits
+    qmb::DevBuf<int64_t> orbit_of_row;        // [n_active]
+
+    qmb::GroupArgs group_args() const {
+        qmb::GroupArgs g;
+        g.L = L;
+        g.G = G;
+        g.n_ext = n_ext;
+        g.structured = structured;
+        g.W = W;
+        g.n_chunks = n_chunks;
+        g.mask = (L == 64) ? ~0ull : ((1ull << L) - 1);
+        g.rot = rot.p;
+        g.tables = tables.p;
+        g.chars = chars_dev.p;
+        return g;
+    }
+    qmb::RepTable rep_table() const {
+        qmb::RepTable t;
+        t.reps = reps.p;
+        t.bucket = bucket.p;
+        t.R = R;
+        t.shift = L - T;
+        return t;
+    }
+};

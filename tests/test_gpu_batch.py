@@ -1,0 +1,86 @@
+"""Batched Lanczos (many coupling sets x many momentum sectors) against
+single-sector FP64 solves and dense FP64 diagonalisation."""
+import numpy as np
+import pytest
+
+import oracle as O
+import qmbcuda_b200 as q
+from helpers import oracle_group, oracle_terms
+
+pytestmark = pytest.mark.gpu
+A = q._capi
+
+
+def _sectors(L):
+    perm, ch = q.translation_group(L)
+    return [q.Sector(L, L // 2, perm).set_irrep(ch[a]) for a in range(L)], perm, ch
+
+
+@pytest.mark.parametrize("mode", [A.MODE_FP64, A.MODE_MIXED])
+def test_batch_matches_single_solves(mode):
+    L, n_sets = 10, 40
+    secs, perm, ch = _sectors(L)
+    bonds = q.chain_bonds(L)
+    b = q.Batch(secs, q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"), n_sets)
+    rng = np.random.default_rng(20261203)
+    delta = rng.uniform(0, 2, n_sets)
+    J = rng.uniform(0.5, 1.5, n_sets)
+    E, summ = b.solve(J, J * delta, mode=mode, max_iter=200, tol=1e-12)
+    assert E.shape == (n_sets, L)
+    for i in (0, 7, n_sets - 1):
+        for a in (0, 3, 5):
+            t = q.xxz_terms(bonds, J[i], J[i] * delta[i])
+            e1 = q.Hamiltonian(secs[a], t).lanczos(tol=1e-13).E0
+            assert abs(E[i, a] - e1) <= 1e-10 * abs(e1), (i, a, E[i, a], e1)
+
+
+def test_batch_dense_oracle_and_hv():
+    import torch
+    L, n_sets = 8, 32
+    secs, perm, ch = _sectors(L)
+    bonds = q.chain_bonds(L)
+    txy, tz = q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z")
+    b = q.Batch(secs, txy, tz, n_sets)
+    J = np.linspace(0.5, 1.5, n_sets)
+    D = np.linspace(0.0, 2.0, n_sets)
+    E, _ = b.solve(J, J * D, mode=A.MODE_FP64, tol=1e-12)
+    g = oracle_group(perm, ch)
+    sec = O.build_sector(g, L // 2)
+    for i in (0, 13, 31):
+        for a in range(L):
+            t = q.xxz_terms(bonds, J[i], J[i] * D[i])
+            rc, ind, val, tr = O.ell_terms(sec, oracle_terms(t), a, 2 * t.n_terms + 1)
+            rows = O.active_rows(sec, a)
+            if len(rows) == 0:
+                continue
+            e = O.ground_energy_dense(O.ell_to_csr(ind, val, tr, rows))
+            assert abs(E[i, a] - e) <= 1e-10 * max(1.0, abs(e))
+    # one batched H*v in FP64 against per-sector products
+    info = b.info
+    off, cp = b.layout()
+    tot = int(off[-1])
+    x = torch.randn(tot, dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    b.hv_dev(x.data_ptr(), y.data_ptr(), A.PREC_FP64)
+    torch.cuda.synchronize()
+    xs, ys = x.cpu().numpy(), y.cpu().numpy()
+    stride = info.set_stride
+    for a in (0, 2):
+        rows = O.active_rows(sec, a)
+        t = q.xxz_terms(bonds, 1.0, 0.0)
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(t), a, 2 * t.n_terms + 1)
+        M = O.ell_to_csr(ind, val, tr, rows)
+        tz1 = q.xxz_terms(bonds, 0.0, 1.0)
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(tz1), a, 2 * tz1.n_terms + 1)
+        Dz = O.ell_to_csr(ind, val, tr, rows)
+        n = len(rows)
+        o = int(off[a])
+        if cp[a]:
+            xv = xs[o:o + 2 * n * stride].view(np.complex128).reshape(n, stride)
+            yv = ys[o:o + 2 * n * stride].view(np.complex128).reshape(n, stride)
+        else:
+            xv = xs[o:o + n * stride].reshape(n, stride)
+            yv = ys[o:o + n * stride].reshape(n, stride)
+        for i in (0, 5):
+            want = J[i] * (M @ xv[:, i]) + J[i] * D[i] * (Dz @ xv[:, i])
+            np.testing.assert_allclose(yv[:, i], want, atol=1e-11 * np.abs(want).max())

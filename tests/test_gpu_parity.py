@@ -1,0 +1,144 @@
+"""GPU parity: tables, matrices and H*v through the C ABI against the oracle.
+
+Bit-exact for integer tables (representatives, orbit map, ELL indices and row
+counts); FP64 values within 1e-13 absolute; FP32 within 2e-6 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import qmbcuda_b200 as q
+from helpers import oracle_group, oracle_terms, sector_cases
+
+pytestmark = pytest.mark.gpu
+
+CASES = sector_cases()
+IDS = [c[0] for c in CASES]
+
+
+def _irreps(chars):
+    n = chars.shape[0]
+    return sorted(set([0, n // 2, n - 1, 1 % n]))
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_representatives_norms_orbit_map(case):
+    name, L, k, perm, chars, flip, _ = case
+    g = oracle_group(perm, chars, flip)
+    sec_o = O.build_sector(g, k)
+    s = q.Sector(L, k, perm, spin_flip=flip)
+    info = s.info
+    assert info.n_states == O.binom(L, k)
+    reps = s.reps()
+    assert np.array_equal(reps, sec_o.reps)
+    assert np.array_equal(s.orbit_map(), sec_o.orbit)
+    for a in _irreps(chars):
+        s.set_irrep(chars[a])
+        nrm = s.norms()
+        np.testing.assert_allclose(nrm, sec_o.norms[:, a], rtol=0, atol=1e-13)
+        act = s.active()
+        assert np.array_equal(act, O.active_rows(sec_o, a))
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_lookup(case):
+    name, L, k, perm, chars, flip, _ = case
+    s = q.Sector(L, k, perm, spin_flip=flip)
+    reps = s.reps()
+    rng = np.random.default_rng(7)
+    states = O.enumerate_sector(L, k)
+    pick = states[rng.integers(0, len(states), 500)]
+    orb, el = s.lookup(pick)
+    g = oracle_group(perm, chars, flip)
+    for t, o, e in zip(pick, orb, el):
+        assert o >= 0
+        r = reps[o]
+        z, gi = divmod(int(e), g.G)
+        assert O.lib().oc_apply(int(t), L, np.ascontiguousarray(g.perm[gi]), z) == r
+    bad = np.array([0, (1 << L) - 1, 1], np.uint64)
+    orb, _ = s.lookup(bad)
+    assert (orb[[0, 1]] == -1).all()
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_ell_reference_layout(case):
+    name, L, k, perm, chars, flip, bonds = case
+    terms = q.xxz_terms(bonds, 1.0 + 0.25j if "chain12_T" == name else 1.0, 0.7)
+    g = oracle_group(perm, chars, flip)
+    sec_o = O.build_sector(g, k)
+    s = q.Sector(L, k, perm, spin_flip=flip)
+    W = 2 * len(bonds) + 1
+    for a in _irreps(chars):
+        s.set_irrep(chars[a])
+        ind, val, tr = q.export_ref(s, terms, W)
+        rc, ind_o, val_o, tr_o = O.ell_terms(sec_o, oracle_terms(terms), a, W)
+        assert rc >= 0
+        assert np.array_equal(tr, tr_o)
+        # compare used slots only (unused ones are zero on both sides)
+        assert np.array_equal(ind, ind_o)
+        np.testing.assert_allclose(val, val_o, rtol=0, atol=1e-13)
+
+
+def test_ell_overflow_is_an_error():
+    p, ch = q.translation_group(10)
+    s = q.Sector(10, 5, p).set_irrep(ch[0])
+    with pytest.raises(q.QMBError) as e:
+        q.export_ref(s, q.xxz_terms(q.chain_bonds(10), 1.0, 1.0), 3)
+    assert e.value.status == q._capi.QMB_ERR_ELL_OVERFLOW
+
+
+def test_nosym_layout_matches_reference_rule():
+    L, k = 10, 5
+    bonds = q.chain_bonds(L)
+    # T_standard-style pair list with unequal weights to exercise the swap
+    ti = np.array([i for i, j in bonds] + [j for i, j in bonds], np.int32)
+    tj = np.array([j for i, j in bonds] + [i for i, j in bonds], np.int32)
+    tv = np.ones(len(ti), np.complex128) * 0.8
+    cap = 4 * len(ti)
+    n_ops = np.zeros(cap, np.int32); codes = np.zeros(2 * cap, np.int32)
+    sites = np.zeros(2 * cap, np.int32); sc = np.zeros(2 * cap); nt = q._capi.C.c_int()
+    P = q._capi.ptr
+    q.check(q.lib().qmb_terms_from_pairs(len(ti), P(ti), P(tj), P(q._capi.cplx_buf(tv)), 1.0, 0.5, 1,
+                                         cap, P(n_ops), P(codes), P(sites), P(sc), q._capi.C.byref(nt)))
+    n = nt.value
+    t = q.TermTable(n_ops[:n], codes[:2 * n].reshape(n, 2), sites[:2 * n].reshape(n, 2),
+                    sc[:2 * n].view(np.complex128))
+    W = 12
+    ind, val, tr = q.export_nosym(L, k, t, W)
+    rc, ind_o, val_o, tr_o = O.ell_nosym(L, k, ti, tj, tv, 1.0, 0.5, W)
+    assert rc >= 0
+    assert np.array_equal(tr, tr_o) and np.array_equal(ind, ind_o)
+    np.testing.assert_allclose(val, val_o, atol=1e-14)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_hv_stored_and_matrix_free(case):
+    name, L, k, perm, chars, flip, bonds = case
+    terms = q.xxz_terms(bonds, 1.0, 0.5)
+    g = oracle_group(perm, chars, flip)
+    sec_o = O.build_sector(g, k)
+    s = q.Sector(L, k, perm, spin_flip=flip)
+    a = 1 % chars.shape[0]
+    s.set_irrep(chars[a])
+    if s.info.n_active == 0:
+        pytest.skip("empty irrep")
+    h = q.Hamiltonian(s, terms)
+    W = 2 * len(bonds) + 1
+    rc, ind_o, val_o, tr_o = O.ell_terms(sec_o, oracle_terms(terms), a, W)
+    A = O.ell_to_csr(ind_o, val_o, tr_o, O.active_rows(sec_o, a))
+    n = A.shape[0]
+    assert h.info.n_rows == n
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n) + (1j * rng.standard_normal(n) if h.info.is_complex else 0)
+    y_o = A @ x
+    y = h.hv_host(x, q._capi.PREC_FP64)
+    np.testing.assert_allclose(y, y_o, rtol=0, atol=1e-12 * np.abs(y_o).max())
+    y32 = h.hv_host(x, q._capi.PREC_FP32)
+    np.testing.assert_allclose(y32, y_o, rtol=0, atol=2e-6 * np.abs(y_o).max())
+    import torch
+    dt = torch.complex128 if h.info.is_complex else torch.float64
+    xd = torch.tensor(x, dtype=dt, device="cuda")
+    yd = torch.zeros_like(xd)
+    h.hv_dev(xd.data_ptr(), yd.data_ptr(), q._capi.PREC_FP64, matrix_free=True)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(yd.cpu().numpy(), y_o, rtol=0, atol=1e-12 * np.abs(y_o).max())

@@ -37,6 +37,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+sys.path.insert(1, os.path.join(ROOT, "oracle"))
 
 METRIC = "Hv/s and HBM GB/s, mixed vs FP64 at |dE0|<1e-9; batched sectors/s"
 SEED = 20261203
@@ -133,7 +134,7 @@ def time_batch_hv(torch, q, b, prec, reps=20):
     y = torch.empty_like(x)
     st = torch.cuda.current_stream()
     sh = st.cuda_stream
-    for _ in range(3):
+    for _ in range(2):
         b.hv_dev(x.data_ptr(), y.data_ptr(), prec, sh)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -153,7 +154,7 @@ def run_batched(args, torch, q, rank, world):
     secs, b = build_batched(q, L, n_sets)
     info = b.info
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device="cuda")
-    opts = dict(mode=A.MODE_MIXED, max_iter=300, tol=1e-12, check_every=10, refine_max_iter=60,
+    opts = dict(mode=A.MODE_MIXED, max_iter=300, tol=1e-12, check_every=10, refine_max_iter=300,
                 seed=SEED)
 
     def solve(mode):
@@ -173,7 +174,10 @@ def run_batched(args, torch, q, rank, world):
             hv_count.append(r.n_hv)
     clocks = clk.summary()
     # FP64 reference solve of the same problems, |dE0| of the mixed result
-    E64, r64 = solve(A.MODE_FP64)
+    if args.no_compare:
+        E64, r64 = E_mix, r
+    else:
+        E64, r64 = solve(A.MODE_FP64)
     rel = np.abs(E_mix - E64) / np.maximum(np.abs(E64), 1e-300)
     # per-kernel H*v times
     hv32_ms = time_batch_hv(torch, q, b, A.PREC_FP32)
@@ -183,7 +187,7 @@ def run_batched(args, torch, q, rank, world):
     value = float(np.mean(hv_count)) * units / (ms * 1e-3)
     # end-to-end through the C ABI from host buffers: sectors, batch, solve
     e2e_t = []
-    for _ in range(max(1, min(3, args.steps))):
+    for _ in range(0 if args.no_compare else max(1, min(3, args.steps))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s2, b2 = build_batched(q, L, n_sets)
@@ -193,7 +197,7 @@ def run_batched(args, torch, q, rank, world):
         b2.close()
         for s in s2:
             s.close()
-    e2e_s = float(np.mean(e2e_t))
+    e2e_s = float(np.mean(e2e_t)) if e2e_t else float("nan")
     out = {
         "workload": "batched: 256 XXZ chains L=20 periodic, Delta~U(0,2), J~U(0.5,1.5) "
                     "(mt19937-64 seed 20261203), all k=0..19 of Sz=0, mixed precision",
@@ -212,6 +216,11 @@ def run_batched(args, torch, q, rank, world):
         "hv_kernel_gbs_fp64": info.bytes_hv_fp64 / (hv64_ms * 1e-3) / 1e9,
         "hv_ratio_fp32_over_fp64": hv64_ms / hv32_ms,
         "max_rel_dE0_mixed_vs_fp64": float(rel.max()),
+        "hv_tuner": {"variant_fp32": int(b.info.variant_fp32), "variant_fp64": int(b.info.variant_fp64),
+                     "ms_fp32": [round(v, 4) for v in b.info.tune_ms_fp32],
+                     "ms_fp64": [round(v, 4) for v in b.info.tune_ms_fp64],
+                     "variants": "(unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4)"},
+        "iters_mixed": [int(r.iters_low), int(r.iters)], "iters_fp64": int(r64.iters),
         "E0_min": float(E_mix.min()),
     }
     roof_bytes = info.bytes_hv_fp32
@@ -292,6 +301,10 @@ def main():
     ap.add_argument("--workload", default="batched", choices=["batched"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--hv-only", action="store_true",
+                    help="time only the batched H*v kernels (small device footprint, for profiling)")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the FP64 comparison solve and the end-to-end repeat")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -322,6 +335,16 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import qmbcuda_b200 as q
 
+    if args.hv_only:
+        secs, b = build_batched(q)
+        for prec in (q._capi.PREC_FP32, q._capi.PREC_FP64):
+            ms = time_batch_hv(torch, q, b, prec, reps=max(1, args.steps))
+            info = b.info
+            byt = info.bytes_hv_fp32 if prec == q._capi.PREC_FP32 else info.bytes_hv_fp64
+            print(json.dumps({"kernel": "k_bhv", "prec": "fp32" if prec == q._capi.PREC_FP32 else "fp64",
+                              "ms": ms, "gbs": byt / (ms * 1e-3) / 1e9,
+                              "tune_ms": list(info.tune_ms_fp32 if prec == q._capi.PREC_FP32 else info.tune_ms_fp64)}))
+        return 0
     if dist:
         dist.barrier()
     res = run_batched(args, torch, q, rank, world)

@@ -343,6 +343,10 @@ typedef struct {
     int rows_per_block;     /* rows of one thread block */
     int sets_per_thread;    /* coupling sets handled by one thread */
     int set_stride;         /* sets per row in the device vector layout (padded) */
+    int variant_fp32;       /* H*v kernel variant chosen by the tuner (-1: not tuned yet) */
+    int variant_fp64;
+    float tune_ms_fp32[4];  /* tuner timings of the variants, ms */
+    float tune_ms_fp64[4];
 } qmb_batch_info;
 
 QMB_API qmb_status qmb_batch_create(const qmb_batch_desc* desc, qmb_batch* out);

@@ -17,26 +17,27 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <type_traits>
 
 #include "qmb_ham.cuh"
 #include "qmb_lanczos.cuh"
 
 namespace qmb {
 
-constexpr int kBWarps = 8;          // warps per block
-constexpr int kBRowsPerWarp = 8;    // rows per warp per tile
-constexpr int kBTile = kBWarps * kBRowsPerWarp;
+constexpr int kBThreads = 256;      // threads per block
+constexpr int kBTile = 32;          // rows per work item
 
 struct BatchArgs {
     int n_sectors;
-    int nsp;                     // padded sets (multiple of 32*SPL)
-    int n_groups;                // set groups of 32*SPL
+    int nsp;                     // padded sets: 32, 64, 128 or 256
+    int n_groups;                // unused (1)
     const int* tile_sector;      // [n_tiles]
     const int* tile_row0;        // [n_tiles]
     const int64_t* sec_elem;     // [n_sectors+1] element offset (rows*nsp)
     const int64_t* sec_nrows;    // [n_sectors]
     const int64_t* row_ptr;      // concatenated CSR row pointers (global entry index)
     const int64_t* row_base;     // [n_sectors] index of the sector's first row in row_ptr
+    const int64_t* row0;         // [n_sectors] index of the sector's first row in the diagonals
     const uint32_t* col;
     const void* val;             // double/double2/float/float2 per sector kind
     const void* dxy;             // diagonal of A  [rows]
@@ -44,209 +45,262 @@ struct BatchArgs {
     const double* cxy;           // [nsp]
     const double* cz;            // [nsp]
     const int* active;           // [n_sectors]
+    int max_tile_entries;        // largest CSR entry count of one work item
 };
 
-// Per sector, real and complex storage live in separate arrays; a kernel
-// launch covers sectors of one kind (kind 0 real, 1 complex).
-template <class V>
-struct VecN {
-    V v[8];
+// SPL consecutive sets of one row: one 4-, 8- or 16-byte access.
+template <class V, int SPL>
+struct alignas(sizeof(V) * SPL) Pack {
+    V v[SPL];
 };
 
-template <class V, class M, int SPL>
-__device__ __forceinline__ void load_sets(const V* __restrict__ p, V (&o)[SPL]) {
-#pragma unroll
-    for (int q = 0; q < SPL; ++q) o[q] = p[q];
-}
-
-// K1 (batched): y = H w_j / beta_j - beta_j v_{j-1}; v_j = w_j / beta_j;
-// alpha partials per (tile, set).  Also plain y = H x when lz == nullptr.
 struct BLz {
     double* alpha;      // [cap][n_prob]
     double* beta;       // [cap+1][n_prob]
     double* partials;   // [n_tiles][nsp]
     int* iter;
     int n_prob;
+    unsigned* sec_ctr;       // [n_sectors] tiles finished in the current kernel
+    const int* sec_tile0;    // [n_sectors]
+    const int* sec_ntiles;   // [n_sectors]
 };
 
-template <class V, int SPL>
-__global__ void __launch_bounds__(kBWarps * 32) k_bhv(BatchArgs a, const int* __restrict__ tiles,
-                                                      int n_tiles, const V* __restrict__ X0,
-                                                      V* __restrict__ Y0, V* __restrict__ vring,
-                                                      int K, BLz lz, const double* __restrict__ ritz,
-                                                      void* psi_v, int lanczos) {
+// Called by every thread of a block after it wrote the partials of one tile
+// of sector s.  The block that finishes the sector's last tile sums the
+// sector's partials in tile order (deterministic) into out[s*nsp + set],
+// optionally as a square root, and resets the sector counter.  Other blocks
+// keep working on later sectors meanwhile.
+__device__ __forceinline__ void sector_tail_reduce(const BatchArgs& a, const BLz& lz, int s,
+                                                   double* __restrict__ out, bool take_sqrt) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned old = atomicAdd(lz.sec_ctr + s, 1u);
+        last = (old == (unsigned)lz.sec_ntiles[s] - 1u);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        const int nsp = a.nsp, t0 = lz.sec_tile0[s], nt = lz.sec_ntiles[s];
+        for (int set = threadIdx.x; set < nsp; set += blockDim.x) {
+            double t = 0.0;
+            for (int k = 0; k < nt; ++k) t += __ldcg(lz.partials + (int64_t)(t0 + k) * nsp + set);
+            out[(int64_t)s * nsp + set] = take_sqrt ? sqrt(t) : t;
+        }
+        if (threadIdx.x == 0) lz.sec_ctr[s] = 0u;
+    }
+    __syncthreads();
+}
+
+// Batched H*v, and with `lanczos` the Lanczos step K1:
+//   y = H w_j / beta_j - beta_j v_{j-1};  v_j = w_j / beta_j;  alpha partials per (tile, set)
+// Thread layout: a row is handled by TPR = nsp/SPL threads (whole warps),
+// thread t owns sets t*SPL .. t*SPL+SPL-1, so every gather of x[col] is one
+// 16-byte access per thread and a contiguous nsp-element run per row.  The
+// block's 256 threads form RG = 256/TPR row groups.  Blocks are persistent
+// and take 32-row work items from a queue in sector order, so the rows in
+// flight (and the vectors they gather) stay within about two sectors, which
+// keeps the gathered x resident in L2.  ctr[0] is the queue head, ctr[1]
+// counts retired blocks; the last block resets both.
+template <class V, int SPL, int UNR, int MINB>
+__global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tiles, unsigned* __restrict__ ctr,
+                                                   const V* __restrict__ X0, V* __restrict__ Y0,
+                                                   V* __restrict__ vring, int K, BLz lz,
+                                                   const double* __restrict__ ritz, void* psi_v,
+                                                   int lanczos) {
     using M = V;
-    __shared__ double red[kBWarps][32 * SPL];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ti = blockIdx.x / a.n_groups;
-    const int grp = blockIdx.x % a.n_groups;
-    if (ti >= n_tiles) return;
-    const int tile = tiles[ti];
-    const int s = a.tile_sector[tile];
-    if (lanczos && !a.active[s]) return;
-    const int64_t nrows = a.sec_nrows[s];
+    using PK = Pack<V, SPL>;
+    __shared__ double red[kBThreads * SPL];
+    __shared__ int s_tile;
+    __shared__ int s_rp[kBTile + 1];
+    __shared__ M s_dx[kBTile], s_dz[kBTile];
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    M* s_val = reinterpret_cast<M*>(s_dyn);                    // [max_tile_entries]
+    uint32_t* s_col = reinterpret_cast<uint32_t*>(s_val + a.max_tile_entries);
     const int nsp = a.nsp;
-    const int set0 = grp * 32 * SPL + lane * SPL;
+    const int TPR = nsp / SPL;
+    const int RG = kBThreads / TPR;
+    const int rg = threadIdx.x / TPR, t = threadIdx.x % TPR, set0 = t * SPL;
+    const int lane = threadIdx.x & 31;
     const int j = lanczos ? *lz.iter : 0;
-    const int64_t eo = a.sec_elem[s];
-    const V* X = X0 + (lanczos ? (int64_t)(j & 1) * a.sec_elem[a.n_sectors] : 0) + eo;
-    V* Y = Y0 + (lanczos ? (int64_t)((j + 1) & 1) * a.sec_elem[a.n_sectors] : 0) + eo;
     const int64_t tot = a.sec_elem[a.n_sectors];
-    V* Vc = lanczos ? vring + (int64_t)(j % K) * tot + eo : nullptr;
-    const V* Vp = lanczos ? vring + (int64_t)((j + K - 1) % K) * tot + eo : nullptr;
     const M* val = reinterpret_cast<const M*>(a.val);
     const M* dxy = reinterpret_cast<const M*>(a.dxy);
     const M* dz = reinterpret_cast<const M*>(a.dz);
-    double cx[SPL], cz[SPL], bj[SPL], inv[SPL], cr[SPL], apar[SPL];
-    const int prob0 = s * nsp + set0;
+    using R = typename Sc<V>::real;
+    R cx[SPL], cz[SPL];
 #pragma unroll
     for (int q = 0; q < SPL; ++q) {
-        cx[q] = a.cxy[set0 + q];
-        cz[q] = a.cz[set0 + q];
-        bj[q] = lanczos ? lz.beta[(int64_t)j * lz.n_prob + prob0 + q] : 1.0;
-        inv[q] = 1.0 / bj[q];
-        cr[q] = ritz ? ritz[(int64_t)j * lz.n_prob + prob0 + q] : 0.0;
-        apar[q] = 0.0;
+        cx[q] = (R)a.cxy[set0 + q];
+        cz[q] = (R)a.cz[set0 + q];
     }
-    const int64_t rb = a.row_base[s];
-    const int r_begin = a.tile_row0[tile] + warp * kBRowsPerWarp;
-    for (int rr = 0; rr < kBRowsPerWarp; ++rr) {
-        const int64_t r = r_begin + rr;
-        if (r >= nrows) break;
-        V acc[SPL];
-#pragma unroll
-        for (int q = 0; q < SPL; ++q) acc[q] = Sc<V>::zero();
-        const int64_t p0 = a.row_ptr[rb + r], p1 = a.row_ptr[rb + r + 1];
-        for (int64_t pc = p0; pc < p1; pc += 32) {
-            int cnt = (int)min((int64_t)32, p1 - pc);
-            uint32_t mc = 0;
-            M mv = Sc<M>::zero();
-            if (lane < cnt) {
-                mc = a.col[pc + lane];
-                mv = val[pc + lane];
-            }
-            for (int k = 0; k < cnt; ++k) {
-                uint32_t c = __shfl_sync(0xffffffffu, mc, k);
-                M v;
-                if constexpr (Sc<M>::cplx) {
-                    v.x = __shfl_sync(0xffffffffu, mv.x, k);
-                    v.y = __shfl_sync(0xffffffffu, mv.y, k);
-                } else {
-                    v = __shfl_sync(0xffffffffu, mv, k);
-                }
-                const V* xp = X + (int64_t)c * nsp + set0;
-                V xv[SPL];
-                load_sets<V, M, SPL>(xp, xv);
-#pragma unroll
-                for (int q = 0; q < SPL; ++q) acc[q] = Sc<V>::fma(v, xv[q], acc[q]);
-            }
-        }
-        V xr[SPL];
-        load_sets<V, M, SPL>(X + r * nsp + set0, xr);
-        const M dx = dxy[rb + r], dzz = dz[rb + r];
-        V vp[SPL];
-        if (lanczos && j > 0) load_sets<V, M, SPL>(Vp + r * nsp + set0, vp);
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(ctr, 1u);
+        __syncthreads();
+        const int tile = s_tile;
+        __syncthreads();
+        if (tile >= n_tiles) break;
+        const int s = a.tile_sector[tile];
+        if (lanczos && !a.active[s]) continue;
+        const int64_t nrows = a.sec_nrows[s];
+        const int64_t eo = a.sec_elem[s];
+        const V* X = X0 + (lanczos ? (int64_t)(j & 1) * tot : 0) + eo;
+        V* Y = Y0 + (lanczos ? (int64_t)((j + 1) & 1) * tot : 0) + eo;
+        V* Vc = lanczos ? vring + (int64_t)(j % K) * tot + eo : nullptr;
+        const V* Vp = lanczos ? vring + (int64_t)((j + K - 1) % K) * tot + eo : nullptr;
+        const int prob0 = s * nsp + set0;
+        R bj[SPL], inv[SPL];
+        double apar[SPL];
 #pragma unroll
         for (int q = 0; q < SPL; ++q) {
-            V hx = Sc<V>::add(Sc<V>::scale(Sc<V>::fma(dx, xr[q], acc[q]), cx[q]),
-                              Sc<V>::scale(Sc<V>::mul(dzz, xr[q]), cz[q]));
-            if (!lanczos) {
-                Y[r * nsp + set0 + q] = hx;
-                continue;
+            const double b = lanczos ? lz.beta[(int64_t)j * lz.n_prob + prob0 + q] : 1.0;
+            bj[q] = (R)b;
+            inv[q] = (R)(1.0 / b);
+            apar[q] = 0.0;
+        }
+        const int64_t rb = a.row_base[s], d0 = a.row0[s];
+        const int64_t r0 = a.tile_row0[tile];
+        const int64_t r_end = min(nrows, r0 + kBTile);
+        const int nr = (int)(r_end - r0);
+        // stage the tile's CSR entries, row pointers and diagonals in shared
+        // memory: one coalesced load instead of a dependent chain per row
+        {
+            const int64_t e0 = a.row_ptr[rb + r0];
+            const int ne = (int)(a.row_ptr[rb + r_end] - e0);
+            for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+                s_col[i] = __ldg(a.col + e0 + i);
+                s_val[i] = __ldg(val + e0 + i);
             }
-            V vj = Sc<V>::scale(xr[q], inv[q]);
-            V y = Sc<V>::scale(hx, inv[q]);
-            if (j > 0) y = Sc<V>::sub(y, Sc<V>::scale(vp[q], bj[q]));
-            Vc[r * nsp + set0 + q] = vj;
-            Y[r * nsp + set0 + q] = y;
-            apar[q] += Sc<V>::re_conj_mul(vj, y);
-            if (psi_v && cr[q] != 0.0) {
-                double* ps = reinterpret_cast<double*>(psi_v);
-                if constexpr (Sc<V>::cplx) {
-                    double2* p2 = reinterpret_cast<double2*>(psi_v) + eo + r * nsp + set0 + q;
-                    double2 t = cvt<double2>(vj);
-                    p2->x += cr[q] * t.x;
-                    p2->y += cr[q] * t.y;
-                } else {
-                    ps[eo + r * nsp + set0 + q] += cr[q] * (double)vj;
-                }
+            for (int i = threadIdx.x; i <= nr; i += blockDim.x) s_rp[i] = (int)(a.row_ptr[rb + r0 + i] - e0);
+            for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+                s_dx[i] = dxy[d0 + r0 + i];
+                s_dz[i] = dz[d0 + r0 + i];
             }
         }
-    }
-    if (!lanczos) return;
+        __syncthreads();
+        for (int64_t r = r0 + rg; r < r_end; r += RG) {
+            V acc[SPL];
 #pragma unroll
-    for (int q = 0; q < SPL; ++q) red[warp][lane * SPL + q] = apar[q];
-    __syncthreads();
-    for (int i = threadIdx.x; i < 32 * SPL; i += blockDim.x) {
-        double t = 0.0;
-        for (int w = 0; w < kBWarps; ++w) t += red[w][i];
-        lz.partials[(int64_t)tile * nsp + grp * 32 * SPL + i] = t;
+            for (int q = 0; q < SPL; ++q) acc[q] = Sc<V>::zero();
+            const int p0 = s_rp[r - r0], p1 = s_rp[r - r0 + 1];
+            for (int k = p0; k < p1; k += UNR) {
+                // issue the (up to) UNR gathers first, then the FMAs
+                PK xv[UNR];
+#pragma unroll
+                for (int u = 0; u < UNR; ++u)
+                    if (k + u < p1) xv[u] = *reinterpret_cast<const PK*>(X + (int64_t)s_col[k + u] * nsp + set0);
+#pragma unroll
+                for (int u = 0; u < UNR; ++u)
+                    if (k + u < p1) {
+                        const M v = s_val[k + u];
+#pragma unroll
+                        for (int q = 0; q < SPL; ++q) acc[q] = Sc<V>::fma(v, xv[u].v[q], acc[q]);
+                    }
+            }
+            const PK xr = *reinterpret_cast<const PK*>(X + r * nsp + set0);
+            const M dx = s_dx[r - r0], dzz = s_dz[r - r0];
+            PK vp, vo, yo;
+            if (lanczos && j > 0) vp = *reinterpret_cast<const PK*>(Vp + r * nsp + set0);
+#pragma unroll
+            for (int q = 0; q < SPL; ++q) {
+                V hx = Sc<V>::add(Sc<V>::scale(Sc<V>::fma(dx, xr.v[q], acc[q]), cx[q]),
+                                  Sc<V>::scale(Sc<V>::mul(dzz, xr.v[q]), cz[q]));
+                if (!lanczos) {
+                    yo.v[q] = hx;
+                    continue;
+                }
+                V vj = Sc<V>::scale(xr.v[q], inv[q]);
+                V y = Sc<V>::scale(hx, inv[q]);
+                if (j > 0) y = Sc<V>::sub(y, Sc<V>::scale(vp.v[q], bj[q]));
+                vo.v[q] = vj;
+                yo.v[q] = y;
+                apar[q] += Sc<V>::re_conj_mul(vj, y);
+                const double crq = (psi_v && ritz) ? ritz[(int64_t)j * lz.n_prob + prob0 + q] : 0.0;
+                if (crq != 0.0) {
+                    const int64_t e = eo + r * nsp + set0 + q;
+                    if constexpr (Sc<V>::cplx) {
+                        double2* p2 = reinterpret_cast<double2*>(psi_v) + e;
+                        double2 tv = cvt<double2>(vj);
+                        p2->x += crq * tv.x;
+                        p2->y += crq * tv.y;
+                    } else {
+                        reinterpret_cast<double*>(psi_v)[e] += crq * (double)vj;
+                    }
+                }
+            }
+            *reinterpret_cast<PK*>(Y + r * nsp + set0) = yo;
+            if (lanczos) *reinterpret_cast<PK*>(Vc + r * nsp + set0) = vo;
+        }
+        if (lanczos) {
+#pragma unroll
+            for (int q = 0; q < SPL; ++q) red[rg * nsp + set0 + q] = apar[q];
+            __syncthreads();
+            for (int i = threadIdx.x; i < nsp; i += blockDim.x) {
+                double tt = 0.0;
+                for (int g = 0; g < RG; ++g) tt += red[g * nsp + i];
+                lz.partials[(int64_t)tile * nsp + i] = tt;
+            }
+            sector_tail_reduce(a, lz, s, lz.alpha + (int64_t)j * lz.n_prob, false);
+        } else {
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned d = atomicAdd(ctr + 1, 1u);
+        if (d == gridDim.x - 1) {
+            ctr[0] = 0u;
+            ctr[1] = 0u;
+            __threadfence();
+        }
     }
 }
 
-// K2 (batched): w_{j+1} = y - alpha_j v_j; ||w_{j+1}||^2 partials.
-template <class V, int SPL>
-__global__ void __launch_bounds__(kBWarps * 32) k_bupdate(BatchArgs a, const int* __restrict__ tiles,
-                                                          int n_tiles, V* __restrict__ W0,
-                                                          const V* __restrict__ vring, int K, BLz lz) {
-    __shared__ double red[kBWarps][32 * SPL];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ti = blockIdx.x / a.n_groups;
-    const int grp = blockIdx.x % a.n_groups;
-    if (ti >= n_tiles) return;
-    const int tile = tiles[ti];
+// K2 (batched): w_{j+1} = y - alpha_j v_j; ||w_{j+1}||^2 partials.  One
+// block per work item, thread t = set t (coalesced [row][set] runs).
+template <class V>
+__global__ void k_bupdate(BatchArgs a, int n_tiles, V* __restrict__ W0, const V* __restrict__ vring,
+                          int K, BLz lz) {
+    const int tile = blockIdx.x;
+    const int set = threadIdx.x;
+    if (tile >= n_tiles) return;
     const int s = a.tile_sector[tile];
     if (!a.active[s]) return;
-    const int64_t nrows = a.sec_nrows[s];
     const int nsp = a.nsp;
-    const int set0 = grp * 32 * SPL + lane * SPL;
     const int j = *lz.iter;
     const int64_t tot = a.sec_elem[a.n_sectors];
     const int64_t eo = a.sec_elem[s];
     V* Y = W0 + (int64_t)((j + 1) & 1) * tot + eo;
     const V* Vc = vring + (int64_t)(j % K) * tot + eo;
-    double al[SPL], acc[SPL];
-#pragma unroll
-    for (int q = 0; q < SPL; ++q) {
-        al[q] = lz.alpha[(int64_t)j * lz.n_prob + s * nsp + set0 + q];
-        acc[q] = 0.0;
-    }
-    const int r_begin = a.tile_row0[tile] + warp * kBRowsPerWarp;
-    for (int rr = 0; rr < kBRowsPerWarp; ++rr) {
-        const int64_t r = r_begin + rr;
-        if (r >= nrows) break;
-#pragma unroll
-        for (int q = 0; q < SPL; ++q) {
-            int64_t e = r * nsp + set0 + q;
-            V y = Sc<V>::sub(Y[e], Sc<V>::scale(Vc[e], al[q]));
+    if (set < nsp) {
+        const double al = lz.alpha[(int64_t)j * lz.n_prob + s * nsp + set];
+        double acc = 0.0;
+        const int64_t r_end = min(a.sec_nrows[s], (int64_t)a.tile_row0[tile] + kBTile);
+        for (int64_t r = a.tile_row0[tile]; r < r_end; ++r) {
+            const int64_t e = r * nsp + set;
+            V y = Sc<V>::sub(Y[e], Sc<V>::scale(Vc[e], al));
             Y[e] = y;
-            acc[q] += Sc<V>::abs2(y);
+            acc += Sc<V>::abs2(y);
         }
+        lz.partials[(int64_t)tile * nsp + set] = acc;
     }
-#pragma unroll
-    for (int q = 0; q < SPL; ++q) red[warp][lane * SPL + q] = acc[q];
-    __syncthreads();
-    for (int i = threadIdx.x; i < 32 * SPL; i += blockDim.x) {
-        double t = 0.0;
-        for (int w = 0; w < kBWarps; ++w) t += red[w][i];
-        lz.partials[(int64_t)tile * nsp + grp * 32 * SPL + i] = t;
-    }
+    sector_tail_reduce(a, lz, s, lz.beta + (int64_t)(j + 1) * lz.n_prob, true);
 }
 
-// Sums the tile partials of every problem in tile order.  what 0: alpha[j],
-// 1: beta[j+1] = sqrt(sum) and the step advances (thread 0).
-__global__ void k_breduce(BatchArgs a, const int* __restrict__ sec_tile0,
-                          const int* __restrict__ sec_ntiles, BLz lz, int what) {
-    const int j = *lz.iter;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < lz.n_prob; p += gridDim.x * blockDim.x) {
-        int s = p / a.nsp, set = p % a.nsp;
-        if (!a.active[s]) continue;
-        double t = 0.0;
-        int t0 = sec_tile0[s], nt = sec_ntiles[s];
-        for (int k = 0; k < nt; ++k) t += lz.partials[(int64_t)(t0 + k) * a.nsp + set];
-        if (what == 0) lz.alpha[(int64_t)j * lz.n_prob + p] = t;
-        else lz.beta[(int64_t)(j + 1) * lz.n_prob + p] = sqrt(t);
-    }
+// ||w0||^2 partials per (tile, set).
+template <class V>
+__global__ void k_bnorm0(BatchArgs a, int n_tiles, const V* __restrict__ W0, BLz lz) {
+    const int tile = blockIdx.x;
+    const int set = threadIdx.x;
+    if (tile >= n_tiles || set >= a.nsp) return;
+    const int s = a.tile_sector[tile];
+    const int nsp = a.nsp;
+    const V* X = W0 + a.sec_elem[s];
+    double acc = 0.0;
+    const int64_t r_end = min(a.sec_nrows[s], (int64_t)a.tile_row0[tile] + kBTile);
+    for (int64_t r = a.tile_row0[tile]; r < r_end; ++r) acc += Sc<V>::abs2(X[r * nsp + set]);
+    lz.partials[(int64_t)tile * nsp + set] = acc;
 }
 
 __global__ void k_badvance(BLz lz) {
@@ -278,41 +332,6 @@ __global__ void k_bstart(BatchArgs a, int64_t tot, int mode, uint64_t seed, cons
     }
 }
 
-// ||w0||^2 partials per (tile, set), reusing the update kernel's layout.
-template <class V, int SPL>
-__global__ void __launch_bounds__(kBWarps * 32) k_bnorm0(BatchArgs a, const int* __restrict__ tiles,
-                                                         int n_tiles, const V* __restrict__ W0, BLz lz) {
-    __shared__ double red[kBWarps][32 * SPL];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ti = blockIdx.x / a.n_groups;
-    const int grp = blockIdx.x % a.n_groups;
-    if (ti >= n_tiles) return;
-    const int tile = tiles[ti];
-    const int s = a.tile_sector[tile];
-    const int64_t nrows = a.sec_nrows[s];
-    const int nsp = a.nsp;
-    const int set0 = grp * 32 * SPL + lane * SPL;
-    const V* X = W0 + a.sec_elem[s];
-    double acc[SPL];
-#pragma unroll
-    for (int q = 0; q < SPL; ++q) acc[q] = 0.0;
-    const int r_begin = a.tile_row0[tile] + warp * kBRowsPerWarp;
-    for (int rr = 0; rr < kBRowsPerWarp; ++rr) {
-        const int64_t r = r_begin + rr;
-        if (r >= nrows) break;
-#pragma unroll
-        for (int q = 0; q < SPL; ++q) acc[q] += Sc<V>::abs2(X[r * nsp + set0 + q]);
-    }
-#pragma unroll
-    for (int q = 0; q < SPL; ++q) red[warp][lane * SPL + q] = acc[q];
-    __syncthreads();
-    for (int i = threadIdx.x; i < 32 * SPL; i += blockDim.x) {
-        double t = 0.0;
-        for (int w = 0; w < kBWarps; ++w) t += red[w][i];
-        lz.partials[(int64_t)tile * nsp + grp * 32 * SPL + i] = t;
-    }
-}
-
 __global__ void k_bbeta0(BatchArgs a, const int* __restrict__ sec_tile0,
                          const int* __restrict__ sec_ntiles, BLz lz) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < lz.n_prob; p += gridDim.x * blockDim.x) {
@@ -327,7 +346,7 @@ __global__ void k_bbeta0(BatchArgs a, const int* __restrict__ sec_tile0,
 
 // Lowest Ritz value of every problem by Sturm bisection on its tridiagonal
 // (m_p steps).  Marks converged problems and deactivates finished sectors.
-__device__ double bis_min(const double* al, const double* be, int n_prob, int p, int m) {
+__device__ double bis_kth(const double* al, const double* be, int n_prob, int p, int m, int kth) {
     double lo = al[p], hi = al[p];
     for (int i = 0; i < m; ++i) {
         double a = al[(int64_t)i * n_prob + p];
@@ -351,69 +370,167 @@ __device__ double bis_min(const double* al, const double* be, int n_prob, int p,
             d = al[(int64_t)i * n_prob + p] - x - e * e / d;
             if (d < 0) ++cnt;
         }
-        if (cnt >= 1) hi = x;
+        if (cnt >= kth + 1) hi = x;
         else lo = x;
         if (hi - lo <= 4.5e-16 * fmax(fabs(lo), fabs(hi))) break;
     }
     return 0.5 * (lo + hi);
 }
 
-__global__ void k_bcheck(BatchArgs a, BLz lz, int nsets, double stall, double tol,
+__device__ double bis_min(const double* al, const double* be, int n_prob, int p, int m) {
+    return bis_kth(al, be, n_prob, p, m, 0);
+}
+
+// Last component of the unit eigenvector of T_m for eigenvalue th: inverse
+// iteration with LDL^T of T - th I (tiny pivots replaced), scratch [i][p].
+__device__ double last_ritz_component(const BLz& lz, int p, int m, double th, double* L,
+                                      double* D, double* x) {
+    const int np = lz.n_prob;
+    double scale = 0.0;
+    for (int i = 0; i < m; ++i) scale = fmax(scale, fabs(lz.alpha[(int64_t)i * np + p] - th));
+    double tiny = 1e-15 * fmax(scale, 1e-300);
+    double d = lz.alpha[p] - th;
+    for (int i = 0; i < m; ++i) {
+        if (i > 0) {
+            double e = lz.beta[(int64_t)i * np + p];
+            double l = e / D[(int64_t)(i - 1) * np + p];
+            L[(int64_t)(i - 1) * np + p] = l;
+            d = lz.alpha[(int64_t)i * np + p] - th - l * e;
+        }
+        if (fabs(d) < tiny) d = d < 0 ? -tiny : tiny;
+        D[(int64_t)i * np + p] = d;
+    }
+    for (int i = 0; i < m; ++i) x[(int64_t)i * np + p] = 1.0;
+    double last = 0.0;
+    for (int it = 0; it < 2; ++it) {
+        for (int i = 1; i < m; ++i)
+            x[(int64_t)i * np + p] -= L[(int64_t)(i - 1) * np + p] * x[(int64_t)(i - 1) * np + p];
+        for (int i = 0; i < m; ++i) x[(int64_t)i * np + p] /= D[(int64_t)i * np + p];
+        for (int i = m - 2; i >= 0; --i)
+            x[(int64_t)i * np + p] -= L[(int64_t)i * np + p] * x[(int64_t)(i + 1) * np + p];
+        double nrm = 0.0;
+        for (int i = 0; i < m; ++i) nrm += x[(int64_t)i * np + p] * x[(int64_t)i * np + p];
+        nrm = sqrt(nrm);
+        for (int i = 0; i < m; ++i) x[(int64_t)i * np + p] /= nrm;
+        last = x[(int64_t)(m - 1) * np + p];
+    }
+    return last;
+}
+
+// Lowest Ritz value of every active problem and its convergence test.  With
+// est = beta_m |s_{m-1}| (residual norm of the Ritz pair) and gap = second
+// minus lowest Ritz value (or gap_in from an earlier phase), a problem has
+// converged when
+//   e_tol > 0:   est^2 / gap <= e_tol |theta| and |theta - theta_prev| <= e_tol |theta|
+//   res_tol > 0: est <= res_tol |theta|
+//   stall > 0:   |theta - theta_prev| <= stall |theta| since the last check
+// or when its Krylov space ends.  Sectors with an unconverged set stay active.
+__global__ void k_bcheck(BatchArgs a, BLz lz, int nsets, double stall, double res_tol, double e_tol,
+                         const double* __restrict__ gap_in, double* __restrict__ gap_out,
                          double* __restrict__ theta, double* __restrict__ theta_prev,
-                         int* __restrict__ msteps, int* __restrict__ conv, int* __restrict__ active_next) {
+                         int* __restrict__ msteps, int* __restrict__ conv, int* __restrict__ active_next,
+                         double* __restrict__ L, double* __restrict__ D, double* __restrict__ x) {
     const int m = *lz.iter;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < lz.n_prob; p += gridDim.x * blockDim.x) {
         int s = p / a.nsp, set = p % a.nsp;
         if (!a.active[s] || conv[p]) continue;
-        msteps[p] = m;
-        double th = bis_min(lz.alpha, lz.beta, lz.n_prob, p, m);
-        double prev = theta_prev[p];
+        // a (near) zero beta ends this problem's Krylov space: truncate there
+        int me = m;
+        bool brk = false;
+        for (int i = max(msteps[p], 1); i <= m; ++i) {
+            double bb = lz.beta[(int64_t)i * lz.n_prob + p];
+            double sc_i = fabs(lz.alpha[(int64_t)(i - 1) * lz.n_prob + p]) + 1e-300;
+            if (!(bb > 1e-13 * sc_i)) { me = i; brk = true; break; }
+        }
+        const bool first = msteps[p] == 0;
+        msteps[p] = me;
+        const double th = bis_min(lz.alpha, lz.beta, lz.n_prob, p, me);
+        const double prev = theta_prev[p];
         theta[p] = th;
-        double sc = fmax(fabs(th), 1e-300);
-        double bm = lz.beta[(int64_t)m * lz.n_prob + p];
-        bool done = (fabs(th - prev) <= stall * sc) || (bm <= 1e-13 * sc);
-        (void)tol;
+        const double sc = fmax(fabs(th), 1e-300);
+        bool done = brk;
+        if (!done) {
+            const double est = lz.beta[(int64_t)me * lz.n_prob + p] *
+                               fabs(last_ritz_component(lz, p, me, th, L, D, x));
+            if (res_tol > 0 && est <= res_tol * sc) done = true;
+            // the gap (to the next Ritz value that is not a ghost copy of theta)
+            // only matters once the residual is small
+            if (!done && est <= 1e-3 * sc && (e_tol > 0 || gap_out)) {
+                double own_gap = 1e-10 * sc;
+                for (int kth = 1; kth < min(me, 5); ++kth) {
+                    double tk = bis_kth(lz.alpha, lz.beta, lz.n_prob, p, me, kth);
+                    if (tk - th > 1e-10 * sc) { own_gap = tk - th; break; }
+                }
+                if (gap_out) gap_out[p] = own_gap;
+                const double gap = gap_in ? fmax(gap_in[p], 1e-10 * sc) : own_gap;
+                // energy bound plus a settled theta (a close level not yet
+                // resolved keeps theta moving while the gap estimate is too large)
+                if (e_tol > 0 && !first && est * est / gap <= e_tol * sc && fabs(th - prev) <= e_tol * sc)
+                    done = true;
+            }
+            // FP32 floor: theta no longer moves and the residual is moderate
+            if (stall > 0 && !first && fabs(th - prev) <= stall * sc && est <= 1e-3 * sc) done = true;
+        }
         conv[p] = done ? 1 : 0;
         theta_prev[p] = th;
         if (!done && set < nsets) atomicOr(active_next + s, 1);
     }
 }
 
-// Ritz coefficients of every problem: inverse iteration on T_m - theta I
-// (LDL^T without pivoting, tiny pivots replaced).  Scratch arrays [i][p].
+// Inverse iteration on T_m - th I (LDL^T without pivoting, tiny pivots
+// replaced) for problem p; adds the unit eigenvector to out[i][p].
+__device__ void add_ritz_vector(const BLz& lz, int p, int m, double th, double* L, double* D,
+                                double* x, double* out) {
+    const int np = lz.n_prob;
+    double scale = 0.0;
+    for (int i = 0; i < m; ++i) scale = fmax(scale, fabs(lz.alpha[(int64_t)i * np + p] - th));
+    double tiny = 1e-15 * fmax(scale, 1e-300);
+    double d = lz.alpha[p] - th;
+    for (int i = 0; i < m; ++i) {
+        if (i > 0) {
+            double e = lz.beta[(int64_t)i * np + p];
+            double l = e / D[(int64_t)(i - 1) * np + p];
+            L[(int64_t)(i - 1) * np + p] = l;
+            d = lz.alpha[(int64_t)i * np + p] - th - l * e;
+        }
+        if (fabs(d) < tiny) d = d < 0 ? -tiny : tiny;
+        D[(int64_t)i * np + p] = d;
+    }
+    for (int i = 0; i < m; ++i) x[(int64_t)i * np + p] = 1.0;
+    for (int it = 0; it < 2; ++it) {
+        for (int i = 1; i < m; ++i)
+            x[(int64_t)i * np + p] -= L[(int64_t)(i - 1) * np + p] * x[(int64_t)(i - 1) * np + p];
+        for (int i = 0; i < m; ++i) x[(int64_t)i * np + p] /= D[(int64_t)i * np + p];
+        for (int i = m - 2; i >= 0; --i)
+            x[(int64_t)i * np + p] -= L[(int64_t)i * np + p] * x[(int64_t)(i + 1) * np + p];
+        double nrm = 0.0;
+        for (int i = 0; i < m; ++i) nrm += x[(int64_t)i * np + p] * x[(int64_t)i * np + p];
+        nrm = sqrt(nrm);
+        double sg = x[p] < 0 ? -1.0 : 1.0;
+        for (int i = 0; i < m; ++i) x[(int64_t)i * np + p] *= sg / nrm;
+    }
+    for (int i = 0; i < m; ++i) out[(int64_t)i * np + p] += x[(int64_t)i * np + p];
+}
+
+// Ritz coefficients of every problem: the lowest Ritz vector plus the Ritz
+// vectors of up to three further Ritz values within 1e-4 |theta| of it
+// (ghost copies, within 1e-10, excluded).  A partner level that close may
+// swap order with the ground state under FP32 rounding; starting the FP64
+// restart from the sum keeps both in its Krylov space.  Scratch arrays [i][p].
 __global__ void k_britz(BLz lz, const int* __restrict__ msteps, const double* __restrict__ theta,
-                        double* __restrict__ L, double* __restrict__ D, double* __restrict__ ritz) {
+                        double* __restrict__ L, double* __restrict__ D, double* __restrict__ x,
+                        double* __restrict__ ritz) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < lz.n_prob; p += gridDim.x * blockDim.x) {
         const int np = lz.n_prob;
         const int m = msteps[p];
         const double th = theta[p];
-        double scale = 0.0;
-        for (int i = 0; i < m; ++i) scale = fmax(scale, fabs(lz.alpha[(int64_t)i * np + p] - th));
-        double tiny = 1e-15 * fmax(scale, 1e-300);
-        double d = lz.alpha[p] - th;
-        for (int i = 0; i < m; ++i) {
-            if (i > 0) {
-                double e = lz.beta[(int64_t)i * np + p];
-                double l = e / D[(int64_t)(i - 1) * np + p];
-                L[(int64_t)(i - 1) * np + p] = l;
-                d = lz.alpha[(int64_t)i * np + p] - th - l * e;
-            }
-            if (fabs(d) < tiny) d = d < 0 ? -tiny : tiny;
-            D[(int64_t)i * np + p] = d;
-        }
-        for (int i = 0; i < m; ++i) ritz[(int64_t)i * np + p] = 1.0;
-        for (int it = 0; it < 2; ++it) {
-            // forward: y_{i+1} = b_{i+1} - l_i y_i
-            for (int i = 1; i < m; ++i)
-                ritz[(int64_t)i * np + p] -= L[(int64_t)(i - 1) * np + p] * ritz[(int64_t)(i - 1) * np + p];
-            for (int i = 0; i < m; ++i) ritz[(int64_t)i * np + p] /= D[(int64_t)i * np + p];
-            for (int i = m - 2; i >= 0; --i)
-                ritz[(int64_t)i * np + p] -= L[(int64_t)i * np + p] * ritz[(int64_t)(i + 1) * np + p];
-            double nrm = 0.0;
-            for (int i = 0; i < m; ++i) nrm += ritz[(int64_t)i * np + p] * ritz[(int64_t)i * np + p];
-            nrm = sqrt(nrm);
-            double sg = ritz[p] < 0 ? -1.0 : 1.0;
-            for (int i = 0; i < m; ++i) ritz[(int64_t)i * np + p] *= sg / nrm;
+        const double sc = fmax(fabs(th), 1e-300);
+        for (int i = 0; i < m; ++i) ritz[(int64_t)i * np + p] = 0.0;
+        add_ritz_vector(lz, p, m, th, L, D, x, ritz);
+        for (int kth = 1; kth < min(m, 4); ++kth) {
+            const double tk = bis_kth(lz.alpha, lz.beta, np, p, m, kth);
+            if (tk - th > 1e-4 * sc) break;
+            if (tk - th > 1e-10 * sc) add_ritz_vector(lz, p, m, tk, L, D, x, ritz);
         }
     }
 }
@@ -454,11 +571,16 @@ struct BKind {
     std::vector<int64_t> sec_elem;     // [n+1]
     std::vector<int> tile_sector, tile_row0, sec_tile0, sec_ntiles;
     DevBuf<int> d_tile_sector, d_tile_row0, d_sec_tile0, d_sec_ntiles, d_tiles, d_active;
-    DevBuf<int64_t> d_sec_elem, d_nrows, d_row_ptr, d_row_base;
+    DevBuf<unsigned> d_ctr;      // work queue head + retired blocks
+    DevBuf<unsigned> d_sec_ctr;  // per-sector finished tiles
+    int variant[2] = {-1, -1};    // tuned k_bhv variant per precision (FP32, FP64)
+    float tune_ms[2][4] = {};
+    DevBuf<int64_t> d_sec_elem, d_nrows, d_row_ptr, d_row_base, d_row0;
     DevBuf<uint32_t> d_col;
     DevBuf<unsigned char> val64, val32, dxy64, dxy32, dz64, dz32;
     int64_t nnz = 0, rows = 0;
     int n_tiles = 0;
+    int max_tile_entries = 1;
 };
 
 struct qmb_batch_s {
@@ -482,6 +604,7 @@ static BatchArgs make_args(const qmb_batch_s* b, const BKind& k) {
     a.sec_nrows = k.d_nrows.p;
     a.row_ptr = k.d_row_ptr.p;
     a.row_base = k.d_row_base.p;
+    a.row0 = k.d_row0.p;
     a.col = k.d_col.p;
     a.val = nullptr;
     a.dxy = nullptr;
@@ -489,52 +612,135 @@ static BatchArgs make_args(const qmb_batch_s* b, const BKind& k) {
     a.cxy = b->cxy.p;
     a.cz = b->cz.p;
     a.active = k.d_active.p;
+    a.max_tile_entries = k.max_tile_entries;
     return a;
 }
 
+// Kernel variants the tuner chooses from: gathers in flight per thread
+// (UNR) and the register budget (MINB resident blocks per SM).
+constexpr int kBVariants = 4;
+
+template <class V, int SPL, int UNR, int MINB>
+static void launch_bhv_v(const BatchArgs& a, BKind& k, const V* x, V* y, V* vring, int K, BLz lz,
+                         const double* ritz, void* psi, int lanczos, cudaStream_t st) {
+    static int grid[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& g = grid[dev & 63];
+    if (g == 0) {
+        int per_sm = 0, sms = 148;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bhv<V, SPL, UNR, MINB>, kBThreads,
+                                                      (size_t)a.max_tile_entries * (sizeof(V) + sizeof(uint32_t)));
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = std::max(1, per_sm) * sms;
+    }
+    const size_t smem = (size_t)a.max_tile_entries * (sizeof(V) + sizeof(uint32_t));
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_bhv<V, SPL, UNR, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_bhv<V, SPL, UNR, MINB><<<std::min(g, k.n_tiles), kBThreads, smem, st>>>(
+        a, k.n_tiles, k.d_ctr.p, x, y, vring, K, lz, ritz, psi, lanczos);
+}
+
 template <class V, int SPL>
-static void launch_bhv(const BatchArgs& a, const BKind& k, const V* x, V* y, V* vring, int K,
+static void launch_bhv(int variant, const BatchArgs& a, BKind& k, const V* x, V* y, V* vring, int K,
                        BLz lz, const double* ritz, void* psi, int lanczos, cudaStream_t st) {
-    int blocks = k.n_tiles * a.n_groups;
-    if (blocks == 0) return;
-    k_bhv<V, SPL><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, x, y, vring, K, lz,
-                                                    ritz, psi, lanczos);
-}
-
-template <class V>
-static void bhv_any(int spl, const BatchArgs& a, const BKind& k, const V* x, V* y, V* vring, int K,
-                    BLz lz, const double* ritz, void* psi, int lanczos, cudaStream_t st) {
-    switch (spl) {
-        case 1: launch_bhv<V, 1>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 2: launch_bhv<V, 2>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 4: launch_bhv<V, 4>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        default: launch_bhv<V, 8>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+    if (k.n_tiles == 0) return;
+    switch (variant) {
+        case 0: launch_bhv_v<V, SPL, 8, 2>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+        case 1: launch_bhv_v<V, SPL, 8, 3>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+        case 2: launch_bhv_v<V, SPL, 4, 3>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+        default: launch_bhv_v<V, SPL, 4, 4>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
     }
 }
 
+// sets per thread: one 16-byte access, at most nsp/32
 template <class V>
-static void bupdate_any(int spl, const BatchArgs& a, const BKind& k, V* w, const V* vring, int K,
-                        BLz lz, cudaStream_t st) {
-    int blocks = k.n_tiles * a.n_groups;
-    if (blocks == 0) return;
-    switch (spl) {
-        case 1: k_bupdate<V, 1><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, vring, K, lz); break;
-        case 2: k_bupdate<V, 2><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, vring, K, lz); break;
-        case 4: k_bupdate<V, 4><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, vring, K, lz); break;
-        default: k_bupdate<V, 8><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, vring, K, lz); break;
-    }
+static int spl_for(int nsp) {
+    int spl = (int)(16 / sizeof(V));
+    while (spl > 1 && nsp / spl < 32) spl /= 2;
+    return spl;
 }
 
 template <class V>
-static void bnorm0_any(int spl, const BatchArgs& a, const BKind& k, const V* w, BLz lz, cudaStream_t st) {
-    int blocks = k.n_tiles * a.n_groups;
-    if (blocks == 0) return;
-    switch (spl) {
-        case 1: k_bnorm0<V, 1><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, lz); break;
-        case 2: k_bnorm0<V, 2><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, lz); break;
-        case 4: k_bnorm0<V, 4><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, lz); break;
-        default: k_bnorm0<V, 8><<<blocks, kBWarps * 32, 0, st>>>(a, k.d_tiles.p, k.n_tiles, w, lz); break;
+static void bhv_variant(int variant, const BatchArgs& a, BKind& k, const V* x, V* y, V* vring, int K,
+                        BLz lz, const double* ritz, void* psi, int lanczos, cudaStream_t st) {
+    const int spl = spl_for<V>(a.nsp);
+    if constexpr (sizeof(V) <= 4)
+        if (spl == 4) return launch_bhv<V, 4>(variant, a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+    if constexpr (sizeof(V) <= 8)
+        if (spl == 2) return launch_bhv<V, 2>(variant, a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+    launch_bhv<V, 1>(variant, a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+}
+
+// Autotuner: times every variant on this batch's own matrices (plain H*v on
+// scratch vectors, best of 3) and keeps the fastest for the precision.
+template <class V>
+static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st) {
+    int& v = k.variant[f64 ? 1 : 0];
+    if (v >= 0) return v;
+    const int64_t tot = k.sec_elem[k.n_sectors];
+    DevBuf<V> x(tot), y(tot);
+    QMB_CUDA_TRY(cudaMemsetAsync(x.p, 0, sizeof(V) * tot, st));
+    BLz lz{nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr};
+    cudaEvent_t e0, e1;
+    QMB_CUDA_TRY(cudaEventCreate(&e0));
+    QMB_CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int arg = 0;
+    for (int c = 0; c < kBVariants; ++c) {
+        bhv_variant<V>(c, a, k, x.p, y.p, nullptr, 1, lz, nullptr, nullptr, 0, st);  // warm
+        float tmin = 1e30f;
+        for (int r = 0; r < 3; ++r) {
+            cudaEventRecord(e0, st);
+            bhv_variant<V>(c, a, k, x.p, y.p, nullptr, 1, lz, nullptr, nullptr, 0, st);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            tmin = std::min(tmin, ms);
+        }
+        k.tune_ms[f64 ? 1 : 0][c] = tmin;
+        if (tmin < best) {
+            best = tmin;
+            arg = c;
+        }
     }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_launch("k_bhv tuning");
+    v = arg;
+    return v;
+}
+
+template <class V>
+static void bhv_any(const BatchArgs& a, BKind& k, const V* x, V* y, V* vring, int K, BLz lz,
+                    const double* ritz, void* psi, int lanczos, cudaStream_t st) {
+    const bool f64 = std::is_same<typename Sc<V>::real, double>::value;
+    const int v = k.variant[f64 ? 1 : 0] >= 0 ? k.variant[f64 ? 1 : 0] : 0;
+    bhv_variant<V>(v, a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+}
+
+template <class V>
+static void bupdate_any(const BatchArgs& a, const BKind& k, V* w, const V* vring, int K, BLz lz,
+                        cudaStream_t st) {
+    if (k.n_tiles == 0) return;
+    k_bupdate<V><<<k.n_tiles, a.nsp, 0, st>>>(a, k.n_tiles, w, vring, K, lz);
+}
+
+template <class V>
+static void bnorm0_any(const BatchArgs& a, const BKind& k, const V* w, BLz lz, cudaStream_t st) {
+    if (k.n_tiles == 0) return;
+    k_bnorm0<V><<<k.n_tiles, a.nsp, 0, st>>>(a, k.n_tiles, w, lz);
+}
+
+// Krylov vectors of vec_bytes each that fit in about half of the free
+// device memory (at most want); 0 when fewer than 16 fit.
+static int krylov_slots(size_t vec_bytes, int want) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
+    size_t n = (size_t)(0.5 * (double)fr) / std::max<size_t>(vec_bytes, 1);
+    if (n < 16) return 0;
+    return (int)std::min<size_t>(n, (size_t)want);
 }
 
 struct BPhase {
@@ -546,16 +752,20 @@ struct BPhase {
 // Batched Lanczos phase over one kind with vectors V (and matrix values of
 // the same precision).  start: 0 splitmix (seed), 2 copy of psi_in (FP64).
 template <class V>
-static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, double stall, int check,
-                         int start, uint64_t seed, const void* psi_in, void* psi_out, bool store,
-                         int& n_hv, cudaStream_t st) {
+static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, double stall, double res_tol,
+                         double e_tol, const double* gap_in, double* gap_out, int check, int start,
+                         uint64_t seed, const void* psi_in, void* psi_out, int store_slots, int& n_hv,
+                         cudaStream_t st) {
     BPhase out;
     const int64_t tot = k.sec_elem[k.n_sectors];
     const int n_prob = k.n_sectors * b->nsp;
     int64_t minrows = INT64_MAX;
     for (auto r : k.nrows) minrows = std::min(minrows, r);
-    const int cap = std::max(1, (int)std::min<int64_t>(max_iter, minrows));
-    const int K = store ? cap + 1 : 2;
+    const int cap = std::max(1, max_iter);
+    (void)minrows;
+    // Krylov basis kept on the device (ring of K vectors); when the phase
+    // runs longer than the ring, the Ritz vector is regenerated instead
+    const int K = store_slots > 2 ? std::min(store_slots, cap + 1) : 2;
     DevBuf<V> wbuf(2 * (size_t)tot), vring((size_t)K * tot);
     DevBuf<double> alpha((size_t)(cap + 1) * n_prob), beta((size_t)(cap + 2) * n_prob),
         partials((size_t)std::max(1, k.n_tiles) * b->nsp), theta(n_prob), theta_prev(n_prob),
@@ -563,6 +773,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     DevBuf<int> iter(1), msteps(n_prob), conv(n_prob), active_next(k.n_sectors);
     QMB_CUDA_TRY(cudaMemsetAsync(theta_prev.p, 0, sizeof(double) * n_prob, st));
     QMB_CUDA_TRY(cudaMemsetAsync(conv.p, 0, sizeof(int) * n_prob, st));
+    QMB_CUDA_TRY(cudaMemsetAsync(msteps.p, 0, sizeof(int) * n_prob, st));
     QMB_CUDA_TRY(cudaMemsetAsync(ritz.p, 0, ritz.n * sizeof(double), st));
     QMB_CUDA_TRY(cudaMemsetAsync(alpha.p, 0, alpha.n * sizeof(double), st));
     QMB_CUDA_TRY(cudaMemsetAsync(beta.p, 0, beta.n * sizeof(double), st));
@@ -572,17 +783,16 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     a.val = f64 ? k.val64.p : k.val32.p;
     a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
     a.dz = f64 ? k.dz64.p : k.dz32.p;
-    BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob};
+    BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob, k.d_sec_ctr.p, k.d_sec_tile0.p, k.d_sec_ntiles.p};
     const int rb = 256, rg = (n_prob + rb - 1) / rb;
+    tuned_variant<V>(a, k, f64, st);
     k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
-    bnorm0_any<V>(b->spl, a, k, wbuf.p, lz, st);
+    bnorm0_any<V>(a, k, wbuf.p, lz, st);
     k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
     check_launch("batch start");
     auto step = [&](cudaStream_t ss) {
-        bhv_any<V>(b->spl, a, k, wbuf.p, wbuf.p, vring.p, K, lz, nullptr, nullptr, 1, ss);
-        k_breduce<<<rg, rb, 0, ss>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz, 0);
-        bupdate_any<V>(b->spl, a, k, wbuf.p, vring.p, K, lz, ss);
-        k_breduce<<<rg, rb, 0, ss>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz, 1);
+        bhv_any<V>(a, k, wbuf.p, wbuf.p, vring.p, K, lz, nullptr, nullptr, 1, ss);
+        bupdate_any<V>(a, k, wbuf.p, vring.p, K, lz, ss);
         k_badvance<<<1, 32, 0, ss>>>(lz);
     };
     cudaGraph_t graph = nullptr;
@@ -605,8 +815,8 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
         done += todo;
         n_hv += todo;
         QMB_CUDA_TRY(cudaMemsetAsync(active_next.p, 0, sizeof(int) * k.n_sectors, st));
-        k_bcheck<<<rg, rb, 0, st>>>(a, lz, b->n_sets, stall, 0.0, theta.p, theta_prev.p, msteps.p,
-                                    conv.p, active_next.p);
+        k_bcheck<<<rg, rb, 0, st>>>(a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p,
+                                    theta_prev.p, msteps.p, conv.p, active_next.p, Ls.p, Ds.p, ritz.p);
         QMB_CUDA_TRY(cudaMemcpyAsync(k.d_active.p, active_next.p, sizeof(int) * k.n_sectors,
                                      cudaMemcpyDeviceToDevice, st));
         active_next.download(act.data(), k.n_sectors, st);
@@ -618,8 +828,9 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     out.steps = done;
     // Ritz vectors (FP64) for the next phase or the caller
     if (psi_out) {
-        k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, ritz.p);
-        if (store) {
+        DevBuf<double> xs((size_t)(cap + 1) * n_prob);
+        k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p);
+        if (K > 2 && done < K) {
             k_bpsi<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, vring.p, K, msteps.p, ritz.p, n_prob,
                                                           psi_out);
         } else {
@@ -627,15 +838,13 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             std::vector<int> all(k.n_sectors, 1);
             k.d_active.upload(all.data(), k.n_sectors, st);
             k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
-            bnorm0_any<V>(b->spl, a, k, wbuf.p, lz, st);
+            bnorm0_any<V>(a, k, wbuf.p, lz, st);
             k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
             // regeneration runs every problem to the longest m; coefficients
             // beyond a problem's own m are zero (k_britz wrote m entries)
             for (int j = 0; j < done; ++j) {
-                bhv_any<V>(b->spl, a, k, wbuf.p, wbuf.p, vring.p, K, lz, ritz.p, psi_out, 1, st);
-                k_breduce<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz, 0);
-                bupdate_any<V>(b->spl, a, k, wbuf.p, vring.p, K, lz, st);
-                k_breduce<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz, 1);
+                bhv_any<V>(a, k, wbuf.p, wbuf.p, vring.p, K, lz, ritz.p, psi_out, 1, st);
+                bupdate_any<V>(a, k, wbuf.p, vring.p, K, lz, st);
                 k_badvance<<<1, 32, 0, st>>>(lz);
                 ++n_hv;
             }
@@ -668,11 +877,11 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
         b->device = d->device;
         b->n_sectors = d->n_sectors;
         b->n_sets = d->n_sets;
-        int spl = 1;
-        while (32 * spl < d->n_sets && spl < 8) spl *= 2;
-        b->spl = spl;
-        b->n_groups = (d->n_sets + 32 * spl - 1) / (32 * spl);
-        b->nsp = b->n_groups * 32 * spl;
+        int nsp = 32;
+        while (nsp < d->n_sets) nsp *= 2;
+        b->nsp = nsp;
+        b->n_groups = 1;
+        b->spl = spl_for<float2>(nsp);
         b->sector_kind.resize(d->n_sectors);
         b->sector_pos.resize(d->n_sectors);
         // per-sector matrices through the single-sector builder
@@ -744,7 +953,7 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
         // assemble the two kinds
         for (int kd = 0; kd < 2; ++kd) {
             BKind& K = b->kind[kd];
-            std::vector<int64_t> row_ptr, row_base;
+            std::vector<int64_t> row_ptr, row_base, row0;
             std::vector<uint32_t> col;
             std::vector<double2> val, dxy, dz;
             K.sec_elem.assign(1, 0);
@@ -759,6 +968,7 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                 K.rows += n;
                 K.sec_elem.push_back(K.sec_elem.back() + n * b->nsp);
                 row_base.push_back((int64_t)row_ptr.size());
+                row0.push_back((int64_t)dxy.size());
                 int64_t eb = (int64_t)col.size();
                 for (int64_t r = 0; r <= n; ++r) row_ptr.push_back(eb + P.row_ptr[r]);
                 col.insert(col.end(), P.col.begin(), P.col.end());
@@ -771,6 +981,9 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                 for (int t = 0; t < nt; ++t) {
                     K.tile_sector.push_back(ks);
                     K.tile_row0.push_back(t * kBTile);
+                    int64_t re = std::min<int64_t>(n, (int64_t)(t + 1) * kBTile);
+                    K.max_tile_entries = std::max<int>(K.max_tile_entries,
+                                                       (int)(P.row_ptr[re] - P.row_ptr[(int64_t)t * kBTile]));
                 }
             }
             if (!K.n_sectors) continue;
@@ -786,10 +999,15 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             up_i(K.d_sec_ntiles, K.sec_ntiles);
             up_i(K.d_tiles, tiles);
             K.d_active.alloc(K.n_sectors);
+            K.d_ctr.alloc(2);
+            K.d_ctr.zero();
+            K.d_sec_ctr.alloc(K.n_sectors);
+            K.d_sec_ctr.zero();
             up_l(K.d_sec_elem, K.sec_elem);
             up_l(K.d_nrows, K.nrows);
             up_l(K.d_row_ptr, row_ptr);
             up_l(K.d_row_base, row_base);
+            up_l(K.d_row0, row0);
             K.d_col.alloc(std::max<size_t>(1, col.size()));
             if (!col.empty()) K.d_col.upload(col.data(), col.size());
             // values in the sector kind's scalar types
@@ -852,6 +1070,13 @@ extern "C" qmb_status qmb_batch_get_info(qmb_batch b, qmb_batch_info* info) {
         info->rows_per_block = kBTile;
         info->sets_per_thread = b->spl;
         info->set_stride = b->nsp;
+        const BKind& kc = b->kind[1].n_sectors ? b->kind[1] : b->kind[0];
+        info->variant_fp32 = kc.variant[0];
+        info->variant_fp64 = kc.variant[1];
+        for (int c = 0; c < 4; ++c) {
+            info->tune_ms_fp32[c] = kc.tune_ms[0][c];
+            info->tune_ms_fp64[c] = kc.tune_ms[1][c];
+        }
     });
 }
 
@@ -883,8 +1108,9 @@ static void batch_hv_kind(qmb_batch_s* b, BKind& k, bool f64, const V* x, V* y, 
     a.val = f64 ? k.val64.p : k.val32.p;
     a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
     a.dz = f64 ? k.dz64.p : k.dz32.p;
-    BLz lz{nullptr, nullptr, nullptr, nullptr, 0};
-    bhv_any<V>(b->spl, a, k, x, y, nullptr, 1, lz, nullptr, nullptr, 0, st);
+    BLz lz{nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr};
+    tuned_variant<V>(a, k, f64, st);
+    bhv_any<V>(a, k, x, y, nullptr, 1, lz, nullptr, nullptr, 0, st);
     check_launch("k_bhv");
 }
 }  // namespace qmb
@@ -941,7 +1167,7 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
         b->cxy.upload(hx.data(), b->nsp, st);
         b->cz.upload(hz.data(), b->nsp, st);
         const int check = o.check_every > 0 ? o.check_every : 10;
-        const double stall64 = o.tol > 0 ? o.tol : 1e-12;
+        const double tol64 = o.tol > 0 ? o.tol : 1e-12;
         int n_hv = 0, it_low = 0, it_tot = 0;
         bool all_conv = true;
         std::vector<double> result(b->n_sectors * (size_t)b->n_sets, 0.0), low(result.size(), 0.0);
@@ -954,19 +1180,20 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
             for (auto r : k.nrows) minrows = std::min(minrows, r);
             BPhase ph;
             if (o.mode == QMB_MODE_FP64) {
-                int cap = (int)std::min<int64_t>(o.max_iter, minrows);
-                bool store = fits_device((size_t)(cap + 4) * tot * (kd ? 16 : 8));
-                ph = kd ? run_bphase<double2>(b, k, true, o.max_iter, stall64, check, 0, o.seed, nullptr, nullptr, store, n_hv, st)
-                        : run_bphase<double>(b, k, true, o.max_iter, stall64, check, 0, o.seed, nullptr, nullptr, store, n_hv, st);
+                ph = kd ? run_bphase<double2>(b, k, true, o.max_iter, 0.0, 0.0, tol64, nullptr, nullptr, check, 0, o.seed, nullptr, nullptr, 0, n_hv, st)
+                        : run_bphase<double>(b, k, true, o.max_iter, 0.0, 0.0, tol64, nullptr, nullptr, check, 0, o.seed, nullptr, nullptr, 0, n_hv, st);
                 it_tot = std::max(it_tot, ph.steps);
                 it_low = it_tot;
             } else {
-                int cap = (int)std::min<int64_t>(o.max_iter, minrows);
-                bool store = fits_device((size_t)(cap + 4) * tot * (kd ? 8 : 4));
                 DevBuf<unsigned char> psi(tot * (kd ? 16 : 8));
-                double stall32 = 2e-7;
-                BPhase p1 = kd ? run_bphase<float2>(b, k, false, o.max_iter, stall32, check, 0, o.seed, nullptr, o.mode == QMB_MODE_MIXED ? psi.p : nullptr, store, n_hv, st)
-                               : run_bphase<float>(b, k, false, o.max_iter, stall32, check, 0, o.seed, nullptr, o.mode == QMB_MODE_MIXED ? psi.p : nullptr, store, n_hv, st);
+                const int slots = o.mode == QMB_MODE_MIXED ? krylov_slots((size_t)tot * (kd ? 8 : 4), o.max_iter + 1) : 0;
+                DevBuf<double> gapb((size_t)k.n_sectors * b->nsp);
+                gapb.zero(st);
+                void* psi_out = o.mode == QMB_MODE_MIXED ? (void*)psi.p : nullptr;
+                // FP32 phase: Ritz pair accurate enough that the FP64 restart
+                // needs few steps (residual or energy bound)
+                BPhase p1 = kd ? run_bphase<float2>(b, k, false, o.max_iter, 0.0, 1e-6, 1e-9, nullptr, gapb.p, check, 0, o.seed, nullptr, psi_out, slots, n_hv, st)
+                               : run_bphase<float>(b, k, false, o.max_iter, 0.0, 1e-6, 1e-9, nullptr, gapb.p, check, 0, o.seed, nullptr, psi_out, slots, n_hv, st);
                 it_low = std::max(it_low, p1.steps);
                 for (int s = 0; s < k.n_sectors; ++s)
                     for (int set = 0; set < b->n_sets; ++set)
@@ -974,11 +1201,9 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                 ph = p1;
                 it_tot = std::max(it_tot, p1.steps);
                 if (o.mode == QMB_MODE_MIXED) {
-                    int m2 = o.refine_max_iter > 0 ? o.refine_max_iter : 60;
-                    int cap2 = (int)std::min<int64_t>(m2, minrows);
-                    bool store2 = fits_device((size_t)(cap2 + 4) * tot * (kd ? 16 : 8));
-                    BPhase p2 = kd ? run_bphase<double2>(b, k, true, m2, stall64, std::min(check, 5), 2, 0, psi.p, nullptr, store2, n_hv, st)
-                                   : run_bphase<double>(b, k, true, m2, stall64, std::min(check, 5), 2, 0, psi.p, nullptr, store2, n_hv, st);
+                    int m2 = o.refine_max_iter > 0 ? o.refine_max_iter : 300;
+                    BPhase p2 = kd ? run_bphase<double2>(b, k, true, m2, 0.0, 0.0, tol64, gapb.p, nullptr, 4, 2, 0, psi.p, nullptr, 0, n_hv, st)
+                                   : run_bphase<double>(b, k, true, m2, 0.0, 0.0, tol64, gapb.p, nullptr, 4, 2, 0, psi.p, nullptr, 0, n_hv, st);
                     it_tot = std::max(it_tot, p1.steps + p2.steps);
                     ph = p2;
                 }

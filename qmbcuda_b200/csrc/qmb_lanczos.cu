@@ -307,6 +307,9 @@ struct PhaseOut {
     double theta = 0.0;
     double est = 0.0;     // residual estimate beta_m |s_{m-1}|
     bool converged = false;
+    bool stalled = false;  // theta stopped moving at the FP32 floor
+    double gap = 0.0;      // theta_2 - theta_1 of the last check
+    std::vector<double> s_start;  // Ritz coefficients of the restart vector
     std::vector<double> a, e, s;
     int n_hv = 0;
 };
@@ -315,7 +318,11 @@ struct PhaseOpts {
     int max_iter = 200;
     int min_iter = 1;
     double tol = 1e-12;       // <= 0: run exactly max_iter steps
-    double stall_tol = 0.0;   // stop when |d theta| < stall_tol*|theta| between checks
+    // stopping tests (any one suffices; all off when tol <= 0):
+    double e_tol = 0.0;       // est^2 / gap <= e_tol |theta|  (energy error bound)
+    double res_tol = 0.0;     // est <= res_tol |theta|        (residual of the Ritz pair)
+    double stall_tol = 0.0;   // |d theta| <= stall_tol |theta| between checks
+    double gap_in = 0.0;      // gap to use instead of theta_2 - theta_1 (> 0)
     int reorth = 0;           // CGS passes
     int check_every = 10;
     bool use_graph = true;
@@ -329,7 +336,7 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
                    DevBuf<V>& wbuf, LzState& st, cudaStream_t s) {
     const int64_t n = op.n;
     PhaseOut out;
-    int cap = std::max(1, (int)std::min<int64_t>(po.max_iter, n));
+    int cap = std::max(1, po.max_iter);
     K = store ? cap + 1 : 2;
     vring.alloc((size_t)K * n);
     wbuf.alloc(2 * (size_t)n);
@@ -414,17 +421,43 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
         out.theta = theta;
         out.est = est;
         out.s = sv;
+        out.s_start = sv;
+        // partner levels within 1e-4 |theta| (ghost copies excluded): their
+        // Ritz vectors join the start of an FP64 restart
+        for (int kth = 1; kth < std::min(done, 4); ++kth) {
+            double tk = tridiag_eig(ha.data(), hb.data() + 1, done, kth);
+            if (tk - theta > 1e-4 * std::max(std::fabs(theta), 1e-300)) break;
+            if (tk - theta > 1e-10 * std::max(std::fabs(theta), 1e-300)) {
+                std::vector<double> sk(done);
+                tridiag_eigvec(ha.data(), hb.data() + 1, done, tk, sk.data());
+                for (int i = 0; i < done; ++i) out.s_start[i] += sk[i];
+            }
+        }
         if (breakdown) {
             out.converged = true;
             break;
         }
+        // gap to the next Ritz value that is not a copy of theta (ghosts)
+        out.gap = 1e-10 * scale;
+        for (int kth = 1; kth < std::min(done, 5); ++kth) {
+            double tk = tridiag_eig(ha.data(), hb.data() + 1, done, kth);
+            if (tk - theta > 1e-10 * scale) {
+                out.gap = tk - theta;
+                break;
+            }
+        }
         if (po.tol > 0 && done >= po.min_iter) {
-            bool res_ok = est <= po.tol * scale;
-            bool dth_ok = have_prev && std::fabs(theta - theta_prev) <= po.tol * scale;
-            bool stall = po.stall_tol > 0 && have_prev &&
+            const double gap = po.gap_in > 0 ? std::max(po.gap_in, 1e-10 * scale) : out.gap;
+            // energy bound plus a settled theta (an unresolved close level
+            // keeps theta moving while the gap estimate is too large)
+            bool e_ok = po.e_tol > 0 && have_prev && est * est / gap <= po.e_tol * scale &&
+                        std::fabs(theta - theta_prev) <= po.e_tol * scale;
+            bool r_ok = po.res_tol > 0 && est <= po.res_tol * scale;
+            bool stall = po.stall_tol > 0 && have_prev && est <= 1e-3 * scale &&
                          std::fabs(theta - theta_prev) <= po.stall_tol * scale;
-            if ((res_ok && dth_ok) || stall) {
-                out.converged = res_ok && dth_ok;
+            if (e_ok || r_ok || stall) {
+                out.converged = true;
+                out.stalled = stall && !(e_ok || r_ok);
                 break;
             }
         }
@@ -443,10 +476,10 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
 template <class Op, class V, class P>
 void ritz_vector(const Op& op, size_t op_smem, const PhaseOut& ph, int start_mode, uint64_t seed,
                  const P* from, bool stored, DevBuf<V>& vring, int K, DevBuf<V>& wbuf,
-                 LzState& st, P* psi, int& n_hv, cudaStream_t s) {
+                 LzState& st, P* psi, int& n_hv, cudaStream_t s, bool for_restart = false) {
     const int64_t n = op.n;
     DevBuf<double> ritz(ph.m);
-    ritz.upload(ph.s.data(), ph.m, s);
+    ritz.upload(for_restart ? ph.s_start.data() : ph.s.data(), ph.m, s);
     if (stored) {
         k_ritz<V, P><<<grid_for(n, 256), 256, 0, s>>>(n, vring.p, ph.m, ritz.p, psi);
         check_launch("k_ritz");
@@ -506,9 +539,10 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     po.max_iter = o.max_iter;
     po.min_iter = std::max(1, o.min_iter);
     po.tol = o.tol;
+    po.e_tol = o.tol;  // FP64: stop on the energy error bound
     po.reorth = o.reorth;
     po.check_every = o.check_every > 0 ? o.check_every : 10;
-    const int cap = std::max(1, (int)std::min<int64_t>(o.max_iter, n));
+    const int cap = std::max(1, o.max_iter);
     int n_hv = 0;
     DevBuf<V64> psi(n);
     double theta = 0.0;
@@ -516,7 +550,8 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     bool conv = false;
     PhaseOut last;
 
-    if (o.mode == QMB_MODE_FP64) {
+    // full FP64 solve from the seeded start vector
+    auto fp64_solve = [&]() {
         bool store = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap + 3) * n);
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
         DevBuf<V64> vr, wb;
@@ -526,14 +561,26 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
         ritz_vector<Op64, V64, V64>(op64, sm64, last, o.start, o.seed, nullptr, store, vr, K, wb, st,
                                     psi.p, n_hv, s);
         theta = last.theta;
-        iters = last.m;
+        iters += last.m;
         conv = last.converged;
+    };
+    if (o.mode == QMB_MODE_FP64) {
+        fp64_solve();
     } else {
         // low phase: FP32 vectors and values, FP64 scalars
+        // FP32 vectors: Ritz values stop improving near 1e-7 relative
         PhaseOpts p1 = po;
-        if (o.mode == QMB_MODE_MIXED) {
-            p1.tol = std::max(o.tol, 1e-6);
-            p1.stall_tol = 2e-7;
+        if (o.tol > 0) {  // tol <= 0 keeps the fixed step count
+            if (o.mode == QMB_MODE_MIXED) {
+                // accurate enough that the FP64 restart needs few steps
+                p1.e_tol = 1e-9;
+                p1.res_tol = 1e-6;
+            } else {
+                // FP32 only: stop at the FP32 floor
+                p1.e_tol = 1e-7;
+                p1.res_tol = 1e-6;
+                p1.stall_tol = 2e-7;
+            }
         }
         bool store = o.reorth > 0 || fits_device(sizeof(V32) * (size_t)(cap + 3) * n);
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
@@ -544,7 +591,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
             ph1 = run_phase<Op32, V32, V64>(op32, sm32, p1, o.start, o.seed, nullptr, store, vr, K, wb, st, s);
             n_hv += ph1.n_hv;
             ritz_vector<Op32, V32, V64>(op32, sm32, ph1, o.start, o.seed, nullptr, store, vr, K, wb,
-                                        st, psi.p, n_hv, s);
+                                        st, psi.p, n_hv, s, o.mode == QMB_MODE_MIXED);
         }
         res->E0_low = ph1.theta;
         res->iters_low = ph1.m;
@@ -555,10 +602,11 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
         if (o.mode == QMB_MODE_MIXED) {
             // FP64 restart from the FP32 Ritz vector
             PhaseOpts p2 = po;
-            p2.max_iter = o.refine_max_iter > 0 ? o.refine_max_iter : 60;
+            p2.max_iter = o.refine_max_iter > 0 ? o.refine_max_iter : 300;
             p2.min_iter = 2;
-            p2.check_every = std::min(po.check_every, 5);
-            int cap2 = std::max(1, (int)std::min<int64_t>(p2.max_iter, n));
+            p2.check_every = 4;
+            p2.gap_in = ph1.gap;
+            int cap2 = std::max(1, p2.max_iter);
             bool store2 = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap2 + 3) * n);
             DevBuf<V64> start(n);
             QMB_CUDA_TRY(cudaMemcpyAsync(start.p, psi.p, sizeof(V64) * n, cudaMemcpyDeviceToDevice, s));
@@ -578,6 +626,17 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     double pn2 = 0;
     res->residual = residual_norm<Op64, V64>(op64, sm64, psi.p, theta, st, s, &pn2);
     ++n_hv;
+    if (o.mode == QMB_MODE_MIXED && o.tol > 0) {
+        // A restart whose Krylov residual estimate is far below the true FP64
+        // residual has stagnated (its start vector lacked the ground state,
+        // e.g. a level pair swapped by FP32 rounding): solve in FP64 instead.
+        const double sc = std::max(std::fabs(theta), 1e-300);
+        if (res->residual > 1e-7 * sc && res->residual > 100.0 * last.est) {
+            fp64_solve();
+            res->residual = residual_norm<Op64, V64>(op64, sm64, psi.p, theta, st, s, &pn2);
+            ++n_hv;
+        }
+    }
     res->residual_ref = res->residual * std::sqrt(pn2) / (double)n;
     QMB_CUDA_TRY(cudaEventRecord(e1, s));
     QMB_CUDA_TRY(cudaEventSynchronize(e1));
@@ -614,7 +673,7 @@ extern "C" void qmb_lanczos_default_opts(qmb_lanczos_opts* o) {
     o->seed = 20261203ull;
     o->check_every = 10;
     o->hv = QMB_HV_STORED;
-    o->refine_max_iter = 60;
+    o->refine_max_iter = 300;
     o->want_vector = 0;
 }
 
@@ -696,7 +755,7 @@ extern "C" qmb_status qmb_lanczos_ref_ell(float* E, int n_iter, int nobv, int ma
         qmb_lanczos_opts o;
         qmb_lanczos_default_opts(&o);
         o.mode = QMB_MODE_FP32;
-        o.max_iter = std::min(n_iter, nobv);
+        o.max_iter = n_iter;
         o.tol = 0.0;
         o.start = QMB_START_CURAND;
         o.seed = (uint64_t)seed;

@@ -36,7 +36,7 @@ def test_chain14_translation_irreps(mode, tol, a):
     r = h.lanczos(mode=mode, max_iter=300, tol=1e-12)
     assert abs(r.E0 - e_ref) <= tol * abs(e_ref), (r.E0, e_ref)
     if mode != A.MODE_FP32:
-        assert r.residual < 1e-6
+        assert r.residual < 1e-5
 
 
 def test_spin_inversion_sectors():

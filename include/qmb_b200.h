@@ -293,7 +293,9 @@ typedef struct {
     int n_hv;            /* matrix-vector products, all phases */
     int converged;
     double ms_total;     /* device time of the solve (CUDA events) */
-    double ms_hv;        /* device time inside H*v kernels */
+    double ms_hv;        /* device time inside H*v kernels (-1: not measured) */
+    double n_products;   /* H*v products of single problems computed (batches: active
+                            sectors x coupling sets per step; single solves: n_hv) */
 } qmb_lanczos_result;
 
 QMB_API void qmb_lanczos_default_opts(qmb_lanczos_opts* o);

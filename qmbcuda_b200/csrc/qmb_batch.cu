@@ -18,6 +18,9 @@
 #include <cstring>
 #include <memory>
 #include <type_traits>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 
 #include "qmb_ham.cuh"
 #include "qmb_lanczos.cuh"
@@ -308,6 +311,73 @@ __global__ void k_badvance(BLz lz) {
 }
 
 // Start vectors (splitmix uniform(-1,1) or a copy) and beta_0 per problem.
+// Per (tile, set) partial sums over a sector's rows of two vectors u, w:
+// E == nullptr: part[0] = Re <u, w>, part[1] = ||u||^2;
+// otherwise:    part[0] = ||w - E u||^2 (E per problem), part[1] = 0.
+template <class V>
+__global__ void k_bdot(BatchArgs a, int n_tiles, const V* __restrict__ u, const V* __restrict__ w,
+                       const double* __restrict__ E, double* __restrict__ part) {
+    const int tile = blockIdx.x;
+    const int set = threadIdx.x;
+    if (tile >= n_tiles || set >= a.nsp) return;
+    const int s = a.tile_sector[tile];
+    const int nsp = a.nsp;
+    const int64_t eo = a.sec_elem[s];
+    const double e = E ? E[s * nsp + set] : 0.0;
+    double p0 = 0.0, p1 = 0.0;
+    const int64_t r_end = min(a.sec_nrows[s], (int64_t)a.tile_row0[tile] + kBTile);
+    for (int64_t r = a.tile_row0[tile]; r < r_end; ++r) {
+        const V uu = u[eo + r * nsp + set], ww = w[eo + r * nsp + set];
+        if (E) {
+            p0 += Sc<V>::abs2(Sc<V>::sub(ww, Sc<V>::scale(uu, e)));
+        } else {
+            p0 += Sc<V>::re_conj_mul(uu, ww);
+            p1 += Sc<V>::abs2(uu);
+        }
+    }
+    const int64_t nt = n_tiles;
+    part[(int64_t)tile * nsp + set] = p0;
+    part[(nt + tile) * nsp + set] = p1;
+}
+
+// Sums the tile partials of every problem in tile order: out[k][p] for k < n_arr.
+__global__ void k_bsum(BatchArgs a, int n_tiles, const int* __restrict__ sec_tile0,
+                       const int* __restrict__ sec_ntiles, const double* __restrict__ part, int n_arr,
+                       int n_prob, double* __restrict__ out) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_prob; p += gridDim.x * blockDim.x) {
+        int s = p / a.nsp, set = p % a.nsp;
+        for (int k = 0; k < n_arr; ++k) {
+            double t = 0.0;
+            for (int i = 0; i < sec_ntiles[s]; ++i)
+                t += part[((int64_t)k * n_tiles + sec_tile0[s] + i) * a.nsp + set];
+            out[(int64_t)k * n_prob + p] = t;
+        }
+    }
+}
+
+// Rayleigh quotient of psi (E = <psi,H psi>/<psi,psi>) from s1, s2 in out.
+__global__ void k_brq_energy(int n_prob, const double* __restrict__ sums, double* __restrict__ E) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_prob; p += gridDim.x * blockDim.x)
+        E[p] = sums[p] / sums[n_prob + p];
+}
+
+// Accept a problem when its FP64 residual r satisfies r^2/gap <= tol |E| and
+// r <= 1e-4 |E|; sectors with an unaccepted set stay active for the restart.
+__global__ void k_brq_accept(BatchArgs a, int n_prob, int nsets, const double* __restrict__ E,
+                             const double* __restrict__ r2, const double* __restrict__ psi2,
+                             const double* __restrict__ gap, double tol, int* __restrict__ ok,
+                             int* __restrict__ active) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_prob; p += gridDim.x * blockDim.x) {
+        int s = p / a.nsp, set = p % a.nsp;
+        double sc = fmax(fabs(E[p]), 1e-300);
+        double r = sqrt(r2[p] / fmax(psi2[p], 1e-300));
+        double g = fmax(gap[p], 1e-10 * sc);
+        bool acc = r <= 1e-4 * sc && r * r / g <= tol * sc;
+        ok[p] = acc ? 1 : 0;
+        if (!acc && set < nsets) atomicOr(active + s, 1);
+    }
+}
+
 template <class V>
 __global__ void k_bstart(BatchArgs a, int64_t tot, int mode, uint64_t seed, const void* from,
                          V* __restrict__ w0) {
@@ -519,7 +589,7 @@ __device__ void add_ritz_vector(const BLz& lz, int p, int m, double th, double* 
 // restart from the sum keeps both in its Krylov space.  Scratch arrays [i][p].
 __global__ void k_britz(BLz lz, const int* __restrict__ msteps, const double* __restrict__ theta,
                         double* __restrict__ L, double* __restrict__ D, double* __restrict__ x,
-                        double* __restrict__ ritz) {
+                        double* __restrict__ ritz, double* __restrict__ gap_out) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < lz.n_prob; p += gridDim.x * blockDim.x) {
         const int np = lz.n_prob;
         const int m = msteps[p];
@@ -527,6 +597,14 @@ __global__ void k_britz(BLz lz, const int* __restrict__ msteps, const double* __
         const double sc = fmax(fabs(th), 1e-300);
         for (int i = 0; i < m; ++i) ritz[(int64_t)i * np + p] = 0.0;
         add_ritz_vector(lz, p, m, th, L, D, x, ritz);
+        if (gap_out) {  // gap to the next Ritz value that is not a ghost copy
+            double g = 1e-10 * sc;
+            for (int kth = 1; kth < min(m, 5); ++kth) {
+                double tk = bis_kth(lz.alpha, lz.beta, np, p, m, kth);
+                if (tk - th > 1e-10 * sc) { g = tk - th; break; }
+            }
+            gap_out[p] = g;
+        }
         for (int kth = 1; kth < min(m, 4); ++kth) {
             const double tk = bis_kth(lz.alpha, lz.beta, np, p, m, kth);
             if (tk - th > 1e-4 * sc) break;
@@ -574,6 +652,7 @@ struct BKind {
     DevBuf<unsigned> d_ctr;      // work queue head + retired blocks
     DevBuf<unsigned> d_sec_ctr;  // per-sector finished tiles
     int variant[2] = {-1, -1};    // tuned k_bhv variant per precision (FP32, FP64)
+    DevBuf<unsigned char> ws_ring, ws_w;  // Lanczos workspace kept between solves
     float tune_ms[2][4] = {};
     DevBuf<int64_t> d_sec_elem, d_nrows, d_row_ptr, d_row_base, d_row0;
     DevBuf<uint32_t> d_col;
@@ -735,18 +814,30 @@ static void bnorm0_any(const BatchArgs& a, const BKind& k, const V* w, BLz lz, c
 
 // Krylov vectors of vec_bytes each that fit in about half of the free
 // device memory (at most want); 0 when fewer than 16 fit.
-static int krylov_slots(size_t vec_bytes, int want) {
+static int krylov_slots(size_t vec_bytes, int want, size_t cached = 0) {
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
+    fr += cached;
     size_t n = (size_t)(0.5 * (double)fr) / std::max<size_t>(vec_bytes, 1);
     if (n < 16) return 0;
     return (int)std::min<size_t>(n, (size_t)want);
+}
+
+// QMB_TRACE=1 prints per-phase steps and times of batched solves to stderr.
+static bool trace_on() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("QMB_TRACE");
+        v = (e && *e && *e != '0') ? 1 : 0;
+    }
+    return v == 1;
 }
 
 struct BPhase {
     std::vector<double> theta;   // [n_prob]
     std::vector<int> msteps, conv;
     int steps = 0;
+    double products = 0;  // sector H*v products computed (active sectors x sets x steps)
 };
 
 // Batched Lanczos phase over one kind with vectors V (and matrix values of
@@ -755,7 +846,7 @@ template <class V>
 static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, double stall, double res_tol,
                          double e_tol, const double* gap_in, double* gap_out, int check, int start,
                          uint64_t seed, const void* psi_in, void* psi_out, int store_slots, int& n_hv,
-                         cudaStream_t st) {
+                         cudaStream_t st, const int* init_active = nullptr) {
     BPhase out;
     const int64_t tot = k.sec_elem[k.n_sectors];
     const int n_prob = k.n_sectors * b->nsp;
@@ -766,7 +857,16 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     // Krylov basis kept on the device (ring of K vectors); when the phase
     // runs longer than the ring, the Ritz vector is regenerated instead
     const int K = store_slots > 2 ? std::min(store_slots, cap + 1) : 2;
-    DevBuf<V> wbuf(2 * (size_t)tot), vring((size_t)K * tot);
+    // workspace cached on the handle (grown on demand, reused by later solves)
+    auto grow = [&](DevBuf<unsigned char>& buf, size_t bytes) {
+        if (buf.n < bytes) {
+            buf.release();
+            buf.alloc(bytes);
+        }
+    };
+    grow(k.ws_w, 2 * (size_t)tot * sizeof(V));
+    grow(k.ws_ring, (size_t)K * tot * sizeof(V));
+    struct View { V* p; } wbuf{reinterpret_cast<V*>(k.ws_w.p)}, vring{reinterpret_cast<V*>(k.ws_ring.p)};
     DevBuf<double> alpha((size_t)(cap + 1) * n_prob), beta((size_t)(cap + 2) * n_prob),
         partials((size_t)std::max(1, k.n_tiles) * b->nsp), theta(n_prob), theta_prev(n_prob),
         ritz((size_t)(cap + 1) * n_prob), Ls((size_t)(cap + 1) * n_prob), Ds((size_t)(cap + 1) * n_prob);
@@ -777,8 +877,13 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     QMB_CUDA_TRY(cudaMemsetAsync(ritz.p, 0, ritz.n * sizeof(double), st));
     QMB_CUDA_TRY(cudaMemsetAsync(alpha.p, 0, alpha.n * sizeof(double), st));
     QMB_CUDA_TRY(cudaMemsetAsync(beta.p, 0, beta.n * sizeof(double), st));
-    std::vector<int> ones(k.n_sectors, 1);
-    k.d_active.upload(ones.data(), k.n_sectors, st);
+    if (init_active) {
+        QMB_CUDA_TRY(cudaMemcpyAsync(k.d_active.p, init_active, sizeof(int) * k.n_sectors,
+                                     cudaMemcpyDeviceToDevice, st));
+    } else {
+        std::vector<int> ones(k.n_sectors, 1);
+        k.d_active.upload(ones.data(), k.n_sectors, st);
+    }
     BatchArgs a = make_args(b, k);
     a.val = f64 ? k.val64.p : k.val32.p;
     a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
@@ -805,6 +910,12 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     cudaGetLastError();
     int done = 0;
     std::vector<int> act(k.n_sectors);
+    std::vector<int> act_prev(k.n_sectors, 1);
+    if (init_active) {
+        QMB_CUDA_TRY(cudaMemcpyAsync(act_prev.data(), init_active, sizeof(int) * k.n_sectors,
+                                     cudaMemcpyDeviceToHost, st));
+        QMB_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     while (done < cap) {
         int todo = std::min(std::max(1, check), cap - done);
         for (int t = 0; t < todo; ++t) {
@@ -812,6 +923,11 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             else step(st);
         }
         check_launch("batch step");
+        {
+            int na = 0;
+            for (int v : act_prev) na += v;
+            out.products += (double)todo * na * b->n_sets;
+        }
         done += todo;
         n_hv += todo;
         QMB_CUDA_TRY(cudaMemsetAsync(active_next.p, 0, sizeof(int) * k.n_sectors, st));
@@ -823,13 +939,19 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
         QMB_CUDA_TRY(cudaStreamSynchronize(st));
         bool any = false;
         for (int v : act) any |= v != 0;
+        act_prev = act;
         if (!any) break;
     }
     out.steps = done;
+    if (trace_on()) {
+        QMB_CUDA_TRY(cudaStreamSynchronize(st));
+        std::fprintf(stderr, "[qmb batch] phase %s: %d steps, ring %d, start %d\n", f64 ? "fp64" : "fp32",
+                     done, K, start);
+    }
     // Ritz vectors (FP64) for the next phase or the caller
     if (psi_out) {
         DevBuf<double> xs((size_t)(cap + 1) * n_prob);
-        k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p);
+        k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p, gap_out);
         if (K > 2 && done < K) {
             k_bpsi<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, vring.p, K, msteps.p, ritz.p, n_prob,
                                                           psi_out);
@@ -847,6 +969,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
                 bupdate_any<V>(a, k, wbuf.p, vring.p, K, lz, st);
                 k_badvance<<<1, 32, 0, st>>>(lz);
                 ++n_hv;
+                out.products += (double)k.n_sectors * b->n_sets;
             }
         }
         check_launch("batch ritz");
@@ -1169,6 +1292,7 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
         const int check = o.check_every > 0 ? o.check_every : 10;
         const double tol64 = o.tol > 0 ? o.tol : 1e-12;
         int n_hv = 0, it_low = 0, it_tot = 0;
+        double products = 0;
         bool all_conv = true;
         std::vector<double> result(b->n_sectors * (size_t)b->n_sets, 0.0), low(result.size(), 0.0);
         for (int kd = 0; kd < 2; ++kd) {
@@ -1184,9 +1308,10 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                         : run_bphase<double>(b, k, true, o.max_iter, 0.0, 0.0, tol64, nullptr, nullptr, check, 0, o.seed, nullptr, nullptr, 0, n_hv, st);
                 it_tot = std::max(it_tot, ph.steps);
                 it_low = it_tot;
+                products += ph.products;
             } else {
                 DevBuf<unsigned char> psi(tot * (kd ? 16 : 8));
-                const int slots = o.mode == QMB_MODE_MIXED ? krylov_slots((size_t)tot * (kd ? 8 : 4), o.max_iter + 1) : 0;
+                const int slots = o.mode == QMB_MODE_MIXED ? krylov_slots((size_t)tot * (kd ? 8 : 4), o.max_iter + 1, k.ws_ring.n) : 0;
                 DevBuf<double> gapb((size_t)k.n_sectors * b->nsp);
                 gapb.zero(st);
                 void* psi_out = o.mode == QMB_MODE_MIXED ? (void*)psi.p : nullptr;
@@ -1195,16 +1320,99 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                 BPhase p1 = kd ? run_bphase<float2>(b, k, false, o.max_iter, 0.0, 1e-6, 1e-9, nullptr, gapb.p, check, 0, o.seed, nullptr, psi_out, slots, n_hv, st)
                                : run_bphase<float>(b, k, false, o.max_iter, 0.0, 1e-6, 1e-9, nullptr, gapb.p, check, 0, o.seed, nullptr, psi_out, slots, n_hv, st);
                 it_low = std::max(it_low, p1.steps);
+                products += p1.products;
                 for (int s = 0; s < k.n_sectors; ++s)
                     for (int set = 0; set < b->n_sets; ++set)
                         low[(size_t)set * b->n_sectors + k.sec_index[s]] = p1.theta[(size_t)s * b->nsp + set];
                 ph = p1;
                 it_tot = std::max(it_tot, p1.steps);
                 if (o.mode == QMB_MODE_MIXED) {
+                    // zero-step check: FP64 Rayleigh quotient and residual of the
+                    // FP32 Ritz vectors; accepted problems need no FP64 steps
+                    const int n_prob = k.n_sectors * b->nsp;
+                    std::vector<double> e_rq(n_prob);
+                    std::vector<int> act(k.n_sectors, 0);
+                    DevBuf<int> act_d(k.n_sectors), ok(n_prob);
+                    {
+                        BatchArgs a = make_args(b, k);
+                        a.val = k.val64.p;
+                        a.dxy = k.dxy64.p;
+                        a.dz = k.dz64.p;
+                        DevBuf<unsigned char> hy(tot * (kd ? 16 : 8));
+                        DevBuf<double> part(2 * (size_t)k.n_tiles * b->nsp), sums(2 * (size_t)n_prob),
+                            Eq(n_prob), r2(2 * (size_t)n_prob);
+                        BLz lz0{nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr};
+                        std::vector<int> ones(k.n_sectors, 1);
+                        k.d_active.upload(ones.data(), k.n_sectors, st);
+                        const int rb2 = 256, rg2 = (n_prob + 255) / 256;
+                        if (kd) {
+                            tuned_variant<double2>(a, k, true, st);
+                            bhv_any<double2>(a, k, (const double2*)psi.p, (double2*)hy.p, nullptr, 1, lz0, nullptr, nullptr, 0, st);
+                            k_bdot<double2><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double2*)psi.p, (const double2*)hy.p, nullptr, part.p);
+                        } else {
+                            tuned_variant<double>(a, k, true, st);
+                            bhv_any<double>(a, k, (const double*)psi.p, (double*)hy.p, nullptr, 1, lz0, nullptr, nullptr, 0, st);
+                            k_bdot<double><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double*)psi.p, (const double*)hy.p, nullptr, part.p);
+                        }
+                        k_bsum<<<rg2, rb2, 0, st>>>(a, k.n_tiles, k.d_sec_tile0.p, k.d_sec_ntiles.p, part.p, 2, n_prob, sums.p);
+                        k_brq_energy<<<rg2, rb2, 0, st>>>(n_prob, sums.p, Eq.p);
+                        if (kd) k_bdot<double2><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double2*)psi.p, (const double2*)hy.p, Eq.p, part.p);
+                        else k_bdot<double><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double*)psi.p, (const double*)hy.p, Eq.p, part.p);
+                        k_bsum<<<rg2, rb2, 0, st>>>(a, k.n_tiles, k.d_sec_tile0.p, k.d_sec_ntiles.p, part.p, 1, n_prob, r2.p);
+                        act_d.zero(st);
+                        k_brq_accept<<<rg2, rb2, 0, st>>>(a, n_prob, b->n_sets, Eq.p, r2.p, sums.p + n_prob, gapb.p, tol64, ok.p, act_d.p);
+                        check_launch("rq check");
+                        Eq.download(e_rq.data(), n_prob, st);
+                        act_d.download(act.data(), k.n_sectors, st);
+                        QMB_CUDA_TRY(cudaStreamSynchronize(st));
+                        if (trace_on()) {
+                            std::vector<double> hr2(n_prob), hs(2 * (size_t)n_prob), hg(n_prob);
+                            std::vector<int> hok(n_prob);
+                            r2.download(hr2.data(), n_prob, st);
+                            sums.download(hs.data(), 2 * (size_t)n_prob, st);
+                            gapb.download(hg.data(), n_prob, st);
+                            ok.download(hok.data(), n_prob, st);
+                            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+                            int hist[8] = {0}, nacc = 0, nact = 0;
+                            double worst = 0;
+                            for (int p = 0; p < n_prob; ++p) {
+                                if (p % b->nsp >= b->n_sets) continue;
+                                double sc = std::max(std::fabs(e_rq[p]), 1e-300);
+                                double r = std::sqrt(hr2[p] / std::max(hs[n_prob + p], 1e-300)) / sc;
+                                int bin = r <= 0 ? 0 : std::min(7, std::max(0, (int)std::floor(-std::log10(r)) - 3));
+                                hist[bin]++;
+                                nacc += hok[p];
+                                worst = std::max(worst, r * r * sc / std::max(hg[p], 1e-300));
+                            }
+                            for (int v : act) nact += v;
+                            std::fprintf(stderr, "[qmb batch] rq check: accepted %d, sectors left %d/%d, worst r^2/gap/|E| %.2e, "
+                                         "r/|E| decades 1e-3..1e-10: %d %d %d %d %d %d %d %d\n",
+                                         nacc, nact, k.n_sectors, worst, hist[0], hist[1], hist[2], hist[3], hist[4],
+                                         hist[5], hist[6], hist[7]);
+                        }
+                        ++n_hv;
+                    }
                     int m2 = o.refine_max_iter > 0 ? o.refine_max_iter : 300;
-                    BPhase p2 = kd ? run_bphase<double2>(b, k, true, m2, 0.0, 0.0, tol64, gapb.p, nullptr, 4, 2, 0, psi.p, nullptr, 0, n_hv, st)
-                                   : run_bphase<double>(b, k, true, m2, 0.0, 0.0, tol64, gapb.p, nullptr, 4, 2, 0, psi.p, nullptr, 0, n_hv, st);
+                    bool any = false;
+                    for (int v : act) any |= v != 0;
+                    BPhase p2;
+                    if (any) {
+                        p2 = kd ? run_bphase<double2>(b, k, true, m2, 0.0, 0.0, tol64, gapb.p, nullptr, 4, 2, 0, psi.p, nullptr, 0, n_hv, st, act_d.p)
+                                : run_bphase<double>(b, k, true, m2, 0.0, 0.0, tol64, gapb.p, nullptr, 4, 2, 0, psi.p, nullptr, 0, n_hv, st, act_d.p);
+                    } else {
+                        p2.theta.assign(n_prob, 0.0);
+                        p2.conv.assign(n_prob, 1);
+                        p2.msteps.assign(n_prob, 0);
+                    }
+                    // sectors that skipped the restart keep the Rayleigh quotient
+                    for (int s = 0; s < k.n_sectors; ++s)
+                        if (!act[s])
+                            for (int set = 0; set < b->nsp; ++set) {
+                                p2.theta[(size_t)s * b->nsp + set] = e_rq[(size_t)s * b->nsp + set];
+                                p2.conv[(size_t)s * b->nsp + set] = 1;
+                            }
                     it_tot = std::max(it_tot, p1.steps + p2.steps);
+                    products += p2.products;
                     ph = p2;
                 }
             }
@@ -1228,6 +1436,7 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
             summary->iters = it_tot;
             summary->iters_low = it_low;
             summary->n_hv = n_hv;
+            summary->n_products = products;
             summary->converged = all_conv ? 1 : 0;
             summary->E0 = *std::min_element(result.begin(), result.end());
             summary->E0_low = o.mode == QMB_MODE_FP64 ? summary->E0 : *std::min_element(low.begin(), low.end());

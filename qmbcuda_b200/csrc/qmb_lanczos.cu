@@ -646,6 +646,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     res->E0 = theta;
     res->iters = iters;
     res->n_hv = n_hv;
+    res->n_products = n_hv;
     res->converged = conv ? 1 : 0;
     if (o.mode == QMB_MODE_FP64) res->E0_low = theta;
     if (coeffs) {

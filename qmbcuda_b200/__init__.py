@@ -3,7 +3,7 @@ with Abelian symmetries) behind a C ABI (include/qmb_b200.h).
 
 The compute path is libqmb_b200.so (hand-written sm_100a CUDA + C++ host
 code); this package binds it with ctypes.  Importing it loads the library and
-fails if it has not been built (`python -m qmbcuda_b200.build`).
+fails if it has not been built (`python qmbcuda_b200/build.py`).
 """
 from . import _capi
 from ._capi import QMBError, check, lib

@@ -150,7 +150,7 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise ImportError(f"{LIB_PATH} is missing: run `python -m qmbcuda_b200.build` "
+            raise ImportError(f"{LIB_PATH} is missing: run `python qmbcuda_b200/build.py` "
                               "(the engine has no fallback implementation)")
         L = C.CDLL(LIB_PATH)
         for name, (rt, at) in SIGNATURES.items():

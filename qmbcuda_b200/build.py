@@ -1,7 +1,10 @@
 """Builds libqmb_b200.so in-tree for sm_100a (nvcc, no JIT).
 
-    python -m qmbcuda_b200.build          # incremental
-    python -m qmbcuda_b200.build --force  # rebuild everything
+    python qmbcuda_b200/build.py          # incremental
+    python qmbcuda_b200/build.py --force  # rebuild everything
+
+(run as a file: importing the package loads the library, which a fresh tree
+does not have yet).
 
 Objects go to qmbcuda_b200/_build/, the shared library to
 qmbcuda_b200/libqmb_b200.so (next to this file, so it travels with the tree).

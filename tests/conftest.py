@@ -23,8 +23,13 @@ def pytest_configure(config):
 def _ensure_built():
     lib = os.path.join(ROOT, "qmbcuda_b200", "libqmb_b200.so")
     if not os.path.exists(lib):
-        from qmbcuda_b200 import build
-        build.build()
+        # by path: importing the package would load the missing library
+        import importlib.util
+        spec = importlib.util.spec_from_file_location(
+            "qmbcuda_b200_build", os.path.join(ROOT, "qmbcuda_b200", "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
     orc = os.path.join(ROOT, "oracle", "libqmb_oracle.so")
     if not os.path.exists(orc):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)

@@ -319,6 +319,31 @@ QMB_API qmb_status qmb_lanczos_ref_ell(float* E, int n_iter, int nobv, int max_t
                                int is_complex, float* krylov_out, int check_eig_state,
                                float* residual);
 
+/* qmb_lanczos_ref_ell without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate GPU memory while they
+ * run -- a serving loop that reserved its memory budget up front, a process
+ * under a hard per-process memory cap, or code beside a pooled allocator that
+ * must not see cudaMalloc/cudaFree (both synchronise the whole device).
+ *
+ * Same arguments and results as qmb_lanczos_ref_ell, plus `stream` (a
+ * cudaStream_t; NULL = the legacy default stream).  All work vectors, the
+ * Lanczos scalars and the reduction scratch live in one static device array
+ * of 12 MiB + 64 KiB per device, fixed when the library's device code is
+ * loaded.  Limits: nobv <= 262144 rows and n_iter <= 1024 steps; larger sizes
+ * return QMB_ERR_INVALID (use qmb_lanczos_ref_ell for them).
+ *
+ * The first call on each device does the set-up (looks up the scratch
+ * address, which loads the device code); make that first call before any
+ * stream capture begins.  The scratch is shared by every call on a device in
+ * this process: calls that overlap on the GPU race on it.  This function
+ * takes a process-wide lock and synchronises `stream` before it returns, so
+ * host threads calling it are serialised. */
+QMB_API qmb_status qmb_lanczos_ref_ell_noalloc(float* E, int n_iter, int nobv, int max_terms,
+                                       long long seed, const uint32_t* ind_dev,
+                                       const void* val_dev, const int16_t* track_dev,
+                                       int is_complex, float* krylov_out, int check_eig_state,
+                                       float* residual, void* stream);
+
 /* ============================================================== batches
  * Many coupling sets over many sectors of one model family:
  *   H(i, s) = c_xy[i] * A_s + c_z[i] * D_s

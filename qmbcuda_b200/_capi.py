@@ -134,6 +134,8 @@ SIGNATURES = {
     "qmb_ground_state": (i32, [vp, vp, i64]),
     "qmb_lanczos_ref_ell": (i32, [P(C.c_float), i32, i32, i32, C.c_longlong, vp, vp, vp, i32,
                                   vp, i32, P(C.c_float)]),
+    "qmb_lanczos_ref_ell_noalloc": (i32, [P(C.c_float), i32, i32, i32, C.c_longlong, vp, vp, vp,
+                                          i32, vp, i32, P(C.c_float), vp]),
     "qmb_batch_create": (i32, [P(BatchDesc), P(vp)]),
     "qmb_batch_destroy": (i32, [vp]),
     "qmb_batch_get_info": (i32, [vp, P(BatchInfo)]),

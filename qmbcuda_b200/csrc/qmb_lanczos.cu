@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 
 #include "qmb_ham.cuh"
 #include "qmb_lanczos.cuh"
@@ -774,5 +775,156 @@ extern "C" qmb_status qmb_lanczos_ref_ell(float* E, int n_iter, int nobv, int ma
         if (krylov_out)
             for (int i = 0; i < n_iter; ++i) krylov_out[i] = i < o.max_iter ? (float)cf[i] : 0.0f;
         if (residual) *residual = check_eig_state ? (float)r.residual_ref : 0.0f;
+    });
+}
+
+// ------------------------------------------------------ no-allocation variant
+// qmb_lanczos_ref_ell_noalloc: the computation of qmb_lanczos_ref_ell with
+// every device buffer carved out of one file-scope static array, for callers
+// that must not allocate device memory while they run: a serving loop that
+// owns its memory budget up front, a process sharing the GPU under a hard
+// memory cap, or code running next to a pooled allocator that must not see
+// cudaMalloc/cudaFree traffic (which synchronises the device).
+namespace qmb {
+namespace {
+
+constexpr int64_t kNaMaxRows = 262144;  // nobv limit
+constexpr int kNaMaxIter = 1024;        // n_iter limit
+constexpr int kNaMaxBlocks = 1024;      // reduction partials per grid
+// vectors: 2 work + 2 basis vectors in FP32 and the FP64 Ritz vector, complex
+constexpr size_t kNaVecBytes = (size_t)kNaMaxRows * (4 * sizeof(float2) + sizeof(double2));
+// scalars: alpha, beta, Ritz coefficients, partials (2 grids), scratch, step, counters
+constexpr size_t kNaScalarBytes = 64 * 1024;
+constexpr size_t kNaScratchBytes = kNaVecBytes + kNaScalarBytes;  // 12 MiB + 64 KiB
+static_assert(sizeof(double) * ((kNaMaxIter + 1) + (kNaMaxIter + 2) + kNaMaxIter + 2 * kNaMaxBlocks + 4) +
+                      64 <= kNaScalarBytes,
+              "scalar region too small");
+
+static __device__ __align__(256) unsigned char g_na_scratch[kNaScratchBytes];
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;                          // one caller at a time per process
+unsigned char* g_na_ptr[kNaMaxDevices] = {};    // symbol address per device
+
+// Once per device, with that device current: the address of the static
+// scratch.  The first call on a device loads this module's device code.
+unsigned char* na_scratch(int dev) {
+    QMB_REQUIRE(dev >= 0 && dev < kNaMaxDevices, QMB_ERR_UNSUPPORTED, "device ordinal beyond 63");
+    if (!g_na_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t ce = cudaGetSymbolAddress(&p, g_na_scratch);
+        if (ce != cudaSuccess || !p) {
+            cudaGetLastError();
+            throw Error{QMB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(ce)};
+        }
+        g_na_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_na_ptr[dev];
+}
+
+template <class V, class P>
+void na_solve(unsigned char* base, const RefEllOp<V>& op, int n_iter, uint64_t seed, cudaStream_t s,
+              double* E, double* coeffs, double* res_ref) {
+    const int64_t n = op.n;
+    const int nb = std::min(lz_blocks(), kNaMaxBlocks);
+    // vector region
+    V* wbuf = reinterpret_cast<V*>(base);
+    V* vring = wbuf + 2 * n;
+    P* psi = reinterpret_cast<P*>(base + (size_t)kNaMaxRows * 4 * sizeof(float2));
+    // scalar region
+    double* sc = reinterpret_cast<double*>(base + kNaVecBytes);
+    LzDev d{};
+    d.alpha = sc;
+    d.beta = d.alpha + (kNaMaxIter + 1);
+    double* ritz = d.beta + (kNaMaxIter + 2);
+    d.partials = ritz + kNaMaxIter;
+    d.scratch = d.partials + 2 * kNaMaxBlocks;
+    d.iter = reinterpret_cast<int*>(d.scratch + 4);
+    d.counter = reinterpret_cast<unsigned*>(d.iter + 4);
+    d.coefs = nullptr;
+    d.cpart = nullptr;
+    const int K = 2;
+    // the reduction counters must start at zero (an interrupted earlier call
+    // may have left them set)
+    QMB_CUDA_TRY(cudaMemsetAsync(d.counter, 0, 2 * sizeof(unsigned), s));
+
+    k_lz_start<V, P><<<nb, kLzBlock, 0, s>>>(n, 1, seed, (const P*)nullptr, wbuf, d);
+    for (int j = 0; j < n_iter; ++j) {
+        k_lz_hv<RefEllOp<V>, V, P><<<nb, kLzBlock, 0, s>>>(op, wbuf, vring, K, d, nullptr, (P*)nullptr);
+        k_lz_update<V><<<nb, kLzBlock, 0, s>>>(n, wbuf, vring, K, d, 1);
+    }
+    check_launch("noalloc lanczos steps");
+    double ha[kNaMaxIter + 1], hb[kNaMaxIter + 2];
+    QMB_CUDA_TRY(cudaMemcpyAsync(ha, d.alpha, sizeof(double) * n_iter, cudaMemcpyDeviceToHost, s));
+    QMB_CUDA_TRY(cudaMemcpyAsync(hb, d.beta, sizeof(double) * (n_iter + 1), cudaMemcpyDeviceToHost, s));
+    QMB_CUDA_TRY(cudaStreamSynchronize(s));
+    int m = n_iter;
+    for (int i = 0; i < n_iter; ++i) {
+        QMB_REQUIRE(std::isfinite(ha[i]), QMB_ERR_INVALID, "non-finite Lanczos coefficient (check the Hamiltonian)");
+        double sc_i = std::fabs(ha[i]) + (i > 0 ? std::fabs(hb[i]) : 0.0) + 1e-300;
+        if (!(hb[i + 1] > 1e-13 * sc_i)) {  // invariant subspace reached
+            m = i + 1;
+            break;
+        }
+    }
+    double theta = tridiag_min_eig(ha, hb + 1, m);
+    double sv[kNaMaxIter], work[4 * kNaMaxIter];
+    int iwork[kNaMaxIter];
+    tridiag_eigvec_ws(ha, hb + 1, m, theta, sv, work, iwork);
+    for (int i = 0; i < n_iter; ++i) coeffs[i] = i < m ? sv[i] : 0.0;
+    *E = theta;
+    if (!res_ref) return;
+    // Ritz vector by regenerating v_0..v_{m-1} (same kernels, same order)
+    QMB_CUDA_TRY(cudaMemcpyAsync(ritz, sv, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    QMB_CUDA_TRY(cudaMemsetAsync(psi, 0, sizeof(P) * n, s));
+    k_lz_start<V, P><<<nb, kLzBlock, 0, s>>>(n, 1, seed, (const P*)nullptr, wbuf, d);
+    for (int j = 0; j < m; ++j) {
+        k_lz_hv<RefEllOp<V>, V, P><<<nb, kLzBlock, 0, s>>>(op, wbuf, vring, K, d, ritz, psi);
+        if (j + 1 < m) k_lz_update<V><<<nb, kLzBlock, 0, s>>>(n, wbuf, vring, K, d, 1);
+    }
+    k_residual<RefEllOp<V>, P><<<nb, kLzBlock, 0, s>>>(op, psi, theta, d);
+    check_launch("noalloc residual");
+    double h[2];
+    QMB_CUDA_TRY(cudaMemcpyAsync(h, d.scratch, sizeof(h), cudaMemcpyDeviceToHost, s));
+    QMB_CUDA_TRY(cudaStreamSynchronize(s));
+    double rn = std::sqrt(h[0] / std::max(h[1], 1e-300));
+    *res_ref = rn * std::sqrt(h[1]) / (double)n;
+}
+
+}  // namespace
+}  // namespace qmb
+
+extern "C" qmb_status qmb_lanczos_ref_ell_noalloc(float* E, int n_iter, int nobv, int max_terms,
+                                                  long long seed, const uint32_t* ind_dev,
+                                                  const void* val_dev, const int16_t* track_dev,
+                                                  int is_complex, float* krylov_out,
+                                                  int check_eig_state, float* residual,
+                                                  void* stream) {
+    return guarded([&] {
+        QMB_REQUIRE(E && ind_dev && val_dev && track_dev, QMB_ERR_INVALID, "null argument");
+        QMB_REQUIRE(nobv >= 1 && max_terms >= 1 && n_iter >= 1, QMB_ERR_INVALID, "bad sizes");
+        QMB_REQUIRE(nobv <= kNaMaxRows, QMB_ERR_INVALID,
+                    "nobv exceeds the 262144 rows of the static scratch (use qmb_lanczos_ref_ell)");
+        QMB_REQUIRE(n_iter <= kNaMaxIter, QMB_ERR_INVALID,
+                    "n_iter exceeds the 1024 steps of the static scratch (use qmb_lanczos_ref_ell)");
+        std::lock_guard<std::mutex> lock(g_na_mutex);
+        int dev = 0;
+        QMB_CUDA_TRY(cudaGetDevice(&dev));
+        unsigned char* base = na_scratch(dev);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        double e0 = 0.0, rr = 0.0;
+        double cf[kNaMaxIter];
+        double* want_res = (residual && check_eig_state) ? &rr : nullptr;
+        if (is_complex) {
+            RefEllOp<float2> op{nobv, max_terms, ind_dev, (const float2*)val_dev, track_dev};
+            na_solve<float2, double2>(base, op, n_iter, (uint64_t)seed, s, &e0, cf, want_res);
+        } else {
+            RefEllOp<float> op{nobv, max_terms, ind_dev, (const float*)val_dev, track_dev};
+            na_solve<float, double>(base, op, n_iter, (uint64_t)seed, s, &e0, cf, want_res);
+        }
+        *E = (float)e0;
+        if (krylov_out)
+            for (int i = 0; i < n_iter; ++i) krylov_out[i] = (float)cf[i];
+        if (residual) *residual = check_eig_state ? (float)rr : 0.0f;
     });
 }

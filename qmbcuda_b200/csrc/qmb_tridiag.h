@@ -20,4 +20,9 @@ double tridiag_eig(const double* a, const double* e, int m, int k);
 // first component is >= 0.
 void tridiag_eigvec(const double* a, const double* e, int m, double theta, double* v);
 
+// tridiag_eigvec with caller-provided workspace (work: 4*m doubles, iwork: m
+// ints); performs no heap allocation.
+void tridiag_eigvec_ws(const double* a, const double* e, int m, double theta, double* v,
+                       double* work, int* iwork);
+
 }  // namespace qmb

@@ -49,6 +49,7 @@ struct BatchArgs {
     const double* cz;            // [nsp]
     const int* active;           // [n_sectors]
     int max_tile_entries;        // largest CSR entry count of one work item
+    int c_stride;                // couplings of sector s at cxy[s * c_stride + set] (0: shared)
 };
 
 // SPL consecutive sets of one row: one 4-, 8- or 16-byte access.
@@ -133,11 +134,6 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tile
     const M* dz = reinterpret_cast<const M*>(a.dz);
     using R = typename Sc<V>::real;
     R cx[SPL], cz[SPL];
-#pragma unroll
-    for (int q = 0; q < SPL; ++q) {
-        cx[q] = (R)a.cxy[set0 + q];
-        cz[q] = (R)a.cz[set0 + q];
-    }
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(ctr, 1u);
         __syncthreads();
@@ -146,6 +142,11 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tile
         if (tile >= n_tiles) break;
         const int s = a.tile_sector[tile];
         if (lanczos && !a.active[s]) continue;
+#pragma unroll
+        for (int q = 0; q < SPL; ++q) {
+            cx[q] = (R)a.cxy[(int64_t)s * a.c_stride + set0 + q];
+            cz[q] = (R)a.cz[(int64_t)s * a.c_stride + set0 + q];
+        }
         const int64_t nrows = a.sec_nrows[s];
         const int64_t eo = a.sec_elem[s];
         const V* X = X0 + (lanczos ? (int64_t)(j & 1) * tot : 0) + eo;
@@ -487,6 +488,60 @@ __device__ double last_ritz_component(const BLz& lz, int p, int m, double th, do
     return last;
 }
 
+// Number of eigenvalues of the m x m tridiagonal (a, b) below x: sign
+// changes of the characteristic-polynomial sequence
+//   P_0 = 1, P_1 = a_0 - x, P_i = (a_{i-1} - x) P_{i-1} - b_{i-1}^2 P_{i-2}
+// (Sturm).  The pair is rescaled by a power of two when it leaves
+// [2^-400, 2^400], which keeps every ratio P_i / P_{i-1} exact; a zero P_i
+// is replaced by a tiny value of the previous sign (ratio +tiny, the usual
+// perturbation of the LDL^T count).  b2[i] = b_i^2 for i >= 1.
+__device__ __forceinline__ int sturm_count_poly(const double* __restrict__ a, const double* __restrict__ b2,
+                                                int m, double x) {
+    double p0 = 1.0, p1 = a[0] - x;
+    if (p1 == 0.0) p1 = 1e-300;
+    int cnt = p1 < 0.0;
+    for (int i = 1; i < m; ++i) {
+        double pn = fma(a[i] - x, p1, -b2[i] * p0);
+        if (pn == 0.0) pn = p1 * 0x1p-200;
+        cnt += (pn < 0.0) != (p1 < 0.0);
+        p0 = p1;
+        p1 = pn;
+        const double s = fabs(p1);
+        if (s > 0x1p400 || s < 0x1p-400) {
+            int e;
+            frexp(p1, &e);
+            p0 = ldexp(p0, -e);
+            p1 = ldexp(p1, -e);
+        }
+    }
+    return cnt;
+}
+
+// k-th smallest eigenvalue (k = 0 lowest) by 33-section: every lane counts at
+// one of 32 interior points of [lo, hi] (count(lo) <= k < count(hi) on entry)
+// and the bracket shrinks to the sub-interval where the count passes k.
+// Stops when the width is <= rtol * max(|lo|, |hi|) + atol or stops shrinking.
+__device__ double warp_kth_eig(const double* a, const double* b2, int m, int k, double lo, double hi,
+                               double rtol, double atol) {
+    const int lane = threadIdx.x & 31;
+    for (int round = 0; round < 64; ++round) {
+        const double w = hi - lo;
+        if (!(w > rtol * fmax(fabs(lo), fabs(hi)) + atol)) break;
+        const double x = lo + w * (double)(lane + 1) * (1.0 / 33.0);
+        const int c = sturm_count_poly(a, b2, m, x);
+        const unsigned ge = __ballot_sync(0xffffffffu, c >= k + 1);
+        const int f = ge ? __ffs(ge) - 1 : 32;
+        const double xf = __shfl_sync(0xffffffffu, x, f < 32 ? f : 31);
+        const double xl = __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0);
+        const double nhi = f < 32 ? xf : hi;
+        const double nlo = f > 0 ? xl : lo;
+        if (!(nhi - nlo < w) || !(nlo < nhi)) break;
+        lo = nlo;
+        hi = nhi;
+    }
+    return 0.5 * (lo + hi);
+}
+
 // Lowest Ritz value of every active problem and its convergence test.  With
 // est = beta_m |s_{m-1}| (residual norm of the Ritz pair) and gap = second
 // minus lowest Ritz value (or gap_in from an earlier phase), a problem has
@@ -495,43 +550,127 @@ __device__ double last_ritz_component(const BLz& lz, int p, int m, double th, do
 //   res_tol > 0: est <= res_tol |theta|
 //   stall > 0:   |theta - theta_prev| <= stall |theta| since the last check
 // or when its Krylov space ends.  Sectors with an unconverged set stay active.
+// One warp per problem: the tridiagonal is staged in shared memory
+// (kCheckArrays arrays of stride m + 2 per warp) and the eigenvalues are
+// found by 33-section over the lanes.
+constexpr int kCheckArrays = 6;
 __global__ void k_bcheck(BatchArgs a, BLz lz, int nsets, double stall, double res_tol, double e_tol,
                          const double* __restrict__ gap_in, double* __restrict__ gap_out,
                          double* __restrict__ theta, double* __restrict__ theta_prev,
                          int* __restrict__ msteps, int* __restrict__ conv, int* __restrict__ active_next,
-                         double* __restrict__ L, double* __restrict__ D, double* __restrict__ x) {
+                         int* __restrict__ open_cnt) {
+    extern __shared__ __align__(16) unsigned char s_chk[];
     const int m = *lz.iter;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < lz.n_prob; p += gridDim.x * blockDim.x) {
-        int s = p / a.nsp, set = p % a.nsp;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int stride = m + 2;
+    double* sa = reinterpret_cast<double*>(s_chk) + (size_t)wib * kCheckArrays * stride;
+    double* sb = sa + stride;    // beta_i
+    double* sb2 = sb + stride;   // beta_i^2
+    double* sL = sb2 + stride;
+    double* sD = sL + stride;
+    double* sx = sD + stride;
+    const int np = lz.n_prob;
+    const int wpb = blockDim.x >> 5;
+    for (int p = blockIdx.x * wpb + wib; p < np; p += gridDim.x * wpb) {
+        const int s = p / a.nsp, set = p % a.nsp;
         if (!a.active[s] || conv[p]) continue;
-        // a (near) zero beta ends this problem's Krylov space: truncate there
-        int me = m;
-        bool brk = false;
-        for (int i = max(msteps[p], 1); i <= m; ++i) {
-            double bb = lz.beta[(int64_t)i * lz.n_prob + p];
-            double sc_i = fabs(lz.alpha[(int64_t)(i - 1) * lz.n_prob + p]) + 1e-300;
-            if (!(bb > 1e-13 * sc_i)) { me = i; brk = true; break; }
+        for (int i = lane; i <= m; i += 32) {
+            if (i < m) sa[i] = lz.alpha[(int64_t)i * np + p];
+            const double bb = lz.beta[(int64_t)i * np + p];
+            sb[i] = bb;
+            sb2[i] = bb * bb;
         }
+        __syncwarp();
+        // a (near) zero beta ends this problem's Krylov space: truncate there
+        const int i0 = max(msteps[p], 1);
+        int me = m;
+        for (int base = i0; base <= m; base += 32) {
+            const int i = base + lane;
+            const bool small = i <= m && !(sb[i] > 1e-13 * (fabs(sa[i - 1]) + 1e-300));
+            const unsigned bal = __ballot_sync(0xffffffffu, small);
+            if (bal) {
+                me = base + __ffs(bal) - 1;
+                break;
+            }
+        }
+        const bool brk = me < m || (me == m && !(sb[m] > 1e-13 * (fabs(sa[m - 1]) + 1e-300)));
         const bool first = msteps[p] == 0;
-        msteps[p] = me;
-        const double th = bis_min(lz.alpha, lz.beta, lz.n_prob, p, me);
+        // Gershgorin bracket of T_me
+        double glo = 1e300, ghi = -1e300;
+        for (int i = lane; i < me; i += 32) {
+            const double r = (i > 0 ? fabs(sb[i]) : 0.0) + (i < me - 1 ? fabs(sb[i + 1]) : 0.0);
+            glo = fmin(glo, sa[i] - r);
+            ghi = fmax(ghi, sa[i] + r);
+        }
+        for (int o = 16; o; o >>= 1) {
+            glo = fmin(glo, __shfl_xor_sync(0xffffffffu, glo, o));
+            ghi = fmax(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
+        }
+        const double span = fmax(fabs(glo), fabs(ghi));
+        glo -= 1e-12 * span + 1e-300;
+        ghi += 1e-12 * span + 1e-300;
+        // theta can only decrease as the Krylov space grows: try a narrow
+        // bracket below the previous value first
         const double prev = theta_prev[p];
-        theta[p] = th;
+        double lo = glo, hi = ghi;
+        if (!first) {
+            const double w = 1e-3 * fmax(fabs(prev), 1e-300);
+            const double x = lane == 0 ? prev - w : prev + 8.0 * 2.2e-16 * fabs(prev) + 1e-300;
+            const int c = lane < 2 ? sturm_count_poly(sa, sb2, me, x) : 0;
+            const int c0 = __shfl_sync(0xffffffffu, c, 0), c1 = __shfl_sync(0xffffffffu, c, 1);
+            const double x0 = __shfl_sync(0xffffffffu, x, 0), x1 = __shfl_sync(0xffffffffu, x, 1);
+            if (c0 == 0 && x0 > lo) lo = x0;
+            if (c1 >= 1 && x1 < hi) hi = x1;
+        }
+        const double th = warp_kth_eig(sa, sb2, me, 0, lo, hi, 4.5e-16, 0.0);
         const double sc = fmax(fabs(th), 1e-300);
         bool done = brk;
+        double own_gap = -1.0;
         if (!done) {
-            const double est = lz.beta[(int64_t)me * lz.n_prob + p] *
-                               fabs(last_ritz_component(lz, p, me, th, L, D, x));
+            double est = 0.0;
+            if (lane == 0) {
+                // last component of the unit eigenvector of T_me for th:
+                // inverse iteration with LDL^T of T - th I (tiny pivots replaced)
+                double scale = 0.0;
+                for (int i = 0; i < me; ++i) scale = fmax(scale, fabs(sa[i] - th));
+                const double tiny = 1e-15 * fmax(scale, 1e-300);
+                double d = sa[0] - th;
+                for (int i = 0; i < me; ++i) {
+                    if (i > 0) {
+                        const double l = sb[i] / sD[i - 1];
+                        sL[i - 1] = l;
+                        d = sa[i] - th - l * sb[i];
+                    }
+                    if (fabs(d) < tiny) d = d < 0 ? -tiny : tiny;
+                    sD[i] = d;
+                }
+                for (int i = 0; i < me; ++i) sx[i] = 1.0;
+                double last = 0.0;
+                for (int it = 0; it < 2; ++it) {
+                    for (int i = 1; i < me; ++i) sx[i] -= sL[i - 1] * sx[i - 1];
+                    for (int i = 0; i < me; ++i) sx[i] /= sD[i];
+                    for (int i = me - 2; i >= 0; --i) sx[i] -= sL[i] * sx[i + 1];
+                    double nrm = 0.0;
+                    for (int i = 0; i < me; ++i) nrm += sx[i] * sx[i];
+                    nrm = sqrt(nrm);
+                    for (int i = 0; i < me; ++i) sx[i] /= nrm;
+                    last = sx[me - 1];
+                }
+                est = sb[me] * fabs(last);
+            }
+            est = __shfl_sync(0xffffffffu, est, 0);
             if (res_tol > 0 && est <= res_tol * sc) done = true;
             // the gap (to the next Ritz value that is not a ghost copy of theta)
             // only matters once the residual is small
             if (!done && est <= 1e-3 * sc && (e_tol > 0 || gap_out)) {
-                double own_gap = 1e-10 * sc;
-                for (int kth = 1; kth < min(me, 5); ++kth) {
-                    double tk = bis_kth(lz.alpha, lz.beta, lz.n_prob, p, me, kth);
-                    if (tk - th > 1e-10 * sc) { own_gap = tk - th; break; }
+                own_gap = 1e-10 * sc;
+                const double xg = th + 1e-10 * sc;
+                const int cg = sturm_count_poly(sa, sb2, me, xg);  // same on every lane
+                if (cg < min(me, 5)) {
+                    const double tk = warp_kth_eig(sa, sb2, me, cg, xg, ghi, 0.0, 1e-7 * (ghi - th));
+                    if (tk - th > 1e-10 * sc) own_gap = tk - th;
                 }
-                if (gap_out) gap_out[p] = own_gap;
                 const double gap = gap_in ? fmax(gap_in[p], 1e-10 * sc) : own_gap;
                 // energy bound plus a settled theta (a close level not yet
                 // resolved keeps theta moving while the gap estimate is too large)
@@ -541,9 +680,70 @@ __global__ void k_bcheck(BatchArgs a, BLz lz, int nsets, double stall, double re
             // FP32 floor: theta no longer moves and the residual is moderate
             if (stall > 0 && !first && fabs(th - prev) <= stall * sc && est <= 1e-3 * sc) done = true;
         }
-        conv[p] = done ? 1 : 0;
-        theta_prev[p] = th;
-        if (!done && set < nsets) atomicOr(active_next + s, 1);
+        if (lane == 0) {
+            msteps[p] = me;
+            theta[p] = th;
+            if (gap_out && own_gap > 0) gap_out[p] = own_gap;
+            conv[p] = done ? 1 : 0;
+            theta_prev[p] = th;
+            if (!done && set < nsets) {
+                atomicOr(active_next + s, 1);
+                if (open_cnt) atomicAdd(open_cnt + s, 1);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Loop control of the device-side Lanczos loop (one block), after the test of
+// one block of `check` steps:
+//  - products += check * sum_s active[s] * weight[s]  (problems stepped),
+//  - active <- active_next, then active_next and open_cnt are cleared,
+//  - the loop continues while a sector is active, another block of steps fits
+//    under `cap`, the compacted continuation would not pay (its cost
+//    sum_s rows_s * 32 * ceil(open_s / 32) above compact_ratio times the
+//    current sum_s active_s * rows_s * nsp) and fewer than max_loops blocks ran.
+struct LoopCtl {
+    int loops;
+    int reason;   // 1 converged, 2 step cap, 3 compaction, 4 loop bound
+    double products;
+};
+__global__ void k_bloop_ctl(cudaGraphConditionalHandle h, int n_sectors, int* __restrict__ active,
+                            int* __restrict__ active_next, int* __restrict__ open_cnt,
+                            const int64_t* __restrict__ nrows, const int* __restrict__ weight, int nsp,
+                            int check, int cap, const int* __restrict__ iter, int max_loops,
+                            double compact_ratio, LoopCtl* __restrict__ ctl) {
+    __shared__ double red[32];
+    double prev_w = 0.0, any = 0.0, cost_now = 0.0, cost_c = 0.0;
+    for (int s = threadIdx.x; s < n_sectors; s += blockDim.x) {
+        const int an = active_next[s];
+        prev_w += (double)active[s] * weight[s];
+        any += an;
+        if (an) {
+            cost_now += (double)nrows[s] * nsp;
+            cost_c += (double)nrows[s] * 32.0 * (double)((open_cnt[s] + 31) / 32);
+        }
+    }
+    prev_w = block_sum(prev_w, red);
+    any = block_sum(any, red);
+    cost_now = block_sum(cost_now, red);
+    cost_c = block_sum(cost_c, red);
+    __syncthreads();
+    for (int s = threadIdx.x; s < n_sectors; s += blockDim.x) {
+        active[s] = active_next[s];
+        active_next[s] = 0;
+        open_cnt[s] = 0;
+    }
+    if (threadIdx.x == 0) {
+        ctl->products += (double)check * prev_w;
+        ctl->loops += 1;
+        int go = 1, reason = 0;
+        if (any == 0.0) { go = 0; reason = 1; }
+        else if (*iter + check > cap) { go = 0; reason = 2; }
+        else if (compact_ratio > 0.0 && cost_c <= compact_ratio * cost_now) { go = 0; reason = 3; }
+        else if (ctl->loops >= max_loops) { go = 0; reason = 4; }
+        ctl->reason = reason;
+        cudaGraphSetConditional(h, go);
     }
 }
 
@@ -613,6 +813,65 @@ __global__ void k_britz(BLz lz, const int* __restrict__ msteps, const double* __
     }
 }
 
+// ------------------------------------------------------ compacted sub-batch
+// The unconverged problems of a phase continue their Lanczos recurrences in a
+// packed layout: virtual sector v holds up to nsp_c problems of base sector
+// vs_base[v], slot q being base set vs_set[v * nsp_c + q] (slots past the
+// real ones repeat the last real problem and start converged).
+
+// dst[v][r][q] = src[vs_base[v]][r][vs_set[v][q]], one block per tile of 32 rows.
+template <class V>
+__global__ void k_bgather_vec(BatchArgs ac, const int* __restrict__ vs_base, const int* __restrict__ vs_set,
+                              const int64_t* __restrict__ sec_elem_b, int nsp_b, const V* __restrict__ src,
+                              V* __restrict__ dst) {
+    const int tile = blockIdx.x;
+    const int v = ac.tile_sector[tile];
+    const int nsp_c = ac.nsp;
+    const int q = threadIdx.x % nsp_c;
+    const int set = vs_set[v * nsp_c + q];
+    const int64_t eb = sec_elem_b[vs_base[v]], ec = ac.sec_elem[v];
+    const int64_t r_end = min(ac.sec_nrows[v], (int64_t)ac.tile_row0[tile] + kBTile);
+    for (int64_t r = ac.tile_row0[tile] + threadIdx.x / nsp_c; r < r_end; r += blockDim.x / nsp_c)
+        dst[ec + r * nsp_c + q] = src[eb + r * nsp_b + set];
+}
+
+// alpha_i (i < j), beta_i (i <= j) and the convergence-test state of the
+// migrated problems.
+__global__ void k_bgather_state(int n_prob_c, int nsp_c, int nsp_b, int n_prob_b, int j,
+                                const int* __restrict__ vs_base, const int* __restrict__ vs_set,
+                                const int* __restrict__ real_c, const double* __restrict__ alpha_b,
+                                const double* __restrict__ beta_b, const double* __restrict__ thp_b,
+                                const int* __restrict__ ms_b, const double* __restrict__ gap_b,
+                                double* __restrict__ alpha_c, double* __restrict__ beta_c,
+                                double* __restrict__ thp_c, int* __restrict__ ms_c, double* __restrict__ gap_c,
+                                int* __restrict__ conv_c) {
+    for (int pc = blockIdx.x * blockDim.x + threadIdx.x; pc < n_prob_c; pc += gridDim.x * blockDim.x) {
+        const int v = pc / nsp_c;
+        const int p = vs_base[v] * nsp_b + vs_set[pc];
+        for (int i = 0; i < j; ++i) alpha_c[(int64_t)i * n_prob_c + pc] = alpha_b[(int64_t)i * n_prob_b + p];
+        for (int i = 0; i <= j; ++i) beta_c[(int64_t)i * n_prob_c + pc] = beta_b[(int64_t)i * n_prob_b + p];
+        thp_c[pc] = thp_b[p];
+        ms_c[pc] = ms_b[p];
+        if (gap_b) gap_c[pc] = gap_b[p];
+        conv_c[pc] = real_c[pc] ? 0 : 1;
+    }
+}
+
+// Results of the real slots back into the base problem arrays.
+__global__ void k_bscatter_state(int n_prob_c, int nsp_c, int nsp_b, const int* __restrict__ vs_base,
+                                 const int* __restrict__ vs_set, const int* __restrict__ real_c,
+                                 const double* __restrict__ th_c, const int* __restrict__ ms_c,
+                                 const int* __restrict__ conv_c, double* __restrict__ th_b,
+                                 int* __restrict__ ms_b, int* __restrict__ conv_b) {
+    for (int pc = blockIdx.x * blockDim.x + threadIdx.x; pc < n_prob_c; pc += gridDim.x * blockDim.x) {
+        if (!real_c[pc]) continue;
+        const int p = vs_base[pc / nsp_c] * nsp_b + vs_set[pc];
+        th_b[p] = th_c[pc];
+        ms_b[p] = ms_c[pc];
+        conv_b[p] = conv_c[pc];
+    }
+}
+
 // psi = sum_{i < m_p} ritz[i][p] v_i over the stored basis (FP64 result).
 template <class V>
 __global__ void k_bpsi(BatchArgs a, int64_t tot, const V* __restrict__ vring, int maxm,
@@ -655,6 +914,7 @@ struct BKind {
     DevBuf<unsigned char> ws_ring, ws_w;  // Lanczos workspace kept between solves
     float tune_ms[2][4] = {};
     DevBuf<int64_t> d_sec_elem, d_nrows, d_row_ptr, d_row_base, d_row0;
+    std::vector<int64_t> h_row_base, h_row0;  // per sector, as on the device
     DevBuf<uint32_t> d_col;
     DevBuf<unsigned char> val64, val32, dxy64, dxy32, dz64, dz32;
     int64_t nnz = 0, rows = 0;
@@ -692,6 +952,7 @@ static BatchArgs make_args(const qmb_batch_s* b, const BKind& k) {
     a.cz = b->cz.p;
     a.active = k.d_active.p;
     a.max_tile_entries = k.max_tile_entries;
+    a.c_stride = 0;
     return a;
 }
 
@@ -840,6 +1101,252 @@ struct BPhase {
     double products = 0;  // sector H*v products computed (active sectors x sets x steps)
 };
 
+// Convergence test of every problem after m steps: one warp per problem,
+// shared memory for the staged tridiagonals.
+static void launch_check(const BatchArgs& a, const BLz& lz, int nsets, double stall, double res_tol,
+                         double e_tol, const double* gap_in, double* gap_out, double* theta,
+                         double* theta_prev, int* msteps, int* conv, int* active_next, int m,
+                         cudaStream_t st, int* open_cnt = nullptr) {
+    const size_t per_warp = sizeof(double) * kCheckArrays * (size_t)(m + 2);
+    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (96u << 10) / per_warp));
+    const size_t smem = per_warp * wpb;
+    if (smem > (48u << 10))
+        cudaFuncSetAttribute(k_bcheck, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int nblk = (lz.n_prob + wpb - 1) / wpb;
+    k_bcheck<<<nblk, 32 * wpb, smem, st>>>(a, lz, nsets, stall, res_tol, e_tol, gap_in, gap_out, theta,
+                                           theta_prev, msteps, conv, active_next, open_cnt);
+}
+
+// Runs blocks of `check` Lanczos steps followed by the convergence test as a
+// device-side loop (a CUDA graph with a conditional WHILE node), from step j0
+// until k_bloop_ctl stops it: no host round trip per block.  `step` enqueues
+// one Lanczos step on a stream.  active holds the sectors stepped in the
+// first block.  Returns the step count reached, the stop reason and the
+// problems stepped.
+struct LoopOut {
+    int done;
+    int reason;
+    double products;
+};
+template <class StepFn>
+static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int nsets, double stall,
+                           double res_tol, double e_tol, const double* gap_in, double* gap_out, double* theta,
+                           double* theta_prev, int* msteps, int* conv, int* active, int* active_next,
+                           const int64_t* d_nrows, const int* d_weight, int n_sectors, int check, int j0,
+                           int cap, double compact_ratio, cudaStream_t st) {
+    LoopOut out{j0, 2, 0.0};
+    if (j0 + check > cap) return out;
+    DevBuf<LoopCtl> ctl(1);
+    DevBuf<int> open_cnt(n_sectors);
+    ctl.zero(st);
+    open_cnt.zero(st);
+    QMB_CUDA_TRY(cudaMemsetAsync(active_next, 0, sizeof(int) * n_sectors, st));
+    const int max_loops = (cap - j0) / check + 1;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    struct GG {
+        cudaGraph_t& g;
+        cudaGraphExec_t& e;
+        ~GG() {
+            if (e) cudaGraphExecDestroy(e);
+            if (g) cudaGraphDestroy(g);
+        }
+    } gg{g, ex};
+    QMB_CUDA_TRY(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    QMB_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    // zero-initialised parameter block (the struct has no default constructor)
+    alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(np_raw);
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    QMB_CUDA_TRY(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    QMB_CUDA_TRY(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (int t = 0; t < check; ++t) step(st);
+    launch_check(a, lz, nsets, stall, res_tol, e_tol, gap_in, gap_out, theta, theta_prev, msteps, conv,
+                 active_next, cap, st, open_cnt.p);
+    k_bloop_ctl<<<1, 256, 0, st>>>(h, n_sectors, active, active_next, open_cnt.p, d_nrows, d_weight, a.nsp,
+                                   check, cap, lz.iter, max_loops, compact_ratio, ctl.p);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &captured);
+    QMB_CUDA_TRY(ce);
+    QMB_CUDA_TRY(cudaGraphInstantiate(&ex, g, 0));
+    QMB_CUDA_TRY(cudaGraphLaunch(ex, st));
+    LoopCtl hc;
+    int it = 0;
+    QMB_CUDA_TRY(cudaMemcpyAsync(&hc, ctl.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    QMB_CUDA_TRY(cudaMemcpyAsync(&it, lz.iter, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QMB_CUDA_TRY(cudaStreamSynchronize(st));
+    out.done = it;
+    out.reason = hc.reason;
+    out.products = hc.products;
+    return out;
+}
+
+// Continues the Lanczos recurrences of the unconverged problems of a phase
+// (K = 2 ring, no Ritz vector wanted) in a compacted sub-batch of 32 slots
+// per virtual sector, from step j up to step cap.  conv_h is the host copy of
+// the base convergence flags after step j.  Results (theta, steps, flags) go
+// back into the base arrays; returns the step count reached.
+template <class V>
+static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_base, const BLz& lz_base,
+                         V* wbuf, V* vring, int j, int cap, double stall, double res_tol, double e_tol,
+                         const double* gap_in, int check, const std::vector<int>& conv_h,
+                         double* theta_b, double* theta_prev_b, int* msteps_b, int* conv_b,
+                         double& products, int& n_hv, cudaStream_t st) {
+    constexpr int NC = 32;
+    const int nsp_b = b->nsp;
+    // virtual sectors
+    std::vector<int> vs_base, vs_set, real;
+    std::vector<int> n_real;
+    for (int s = 0; s < k.n_sectors; ++s) {
+        std::vector<int> open;
+        for (int set = 0; set < b->n_sets; ++set)
+            if (!conv_h[(size_t)s * nsp_b + set]) open.push_back(set);
+        for (size_t c = 0; c < open.size(); c += NC) {
+            vs_base.push_back(s);
+            const int nr = (int)std::min<size_t>(NC, open.size() - c);
+            n_real.push_back(nr);
+            for (int q = 0; q < NC; ++q) {
+                vs_set.push_back(open[c + std::min(q, nr - 1)]);
+                real.push_back(q < nr ? 1 : 0);
+            }
+        }
+    }
+    const int nv = (int)vs_base.size();
+    if (nv == 0) return j;
+    BKind ck;
+    ck.n_sectors = nv;
+    ck.variant[0] = k.variant[0];
+    ck.variant[1] = k.variant[1];
+    ck.max_tile_entries = k.max_tile_entries;
+    std::vector<int64_t> rb(nv), r0(nv);
+    ck.sec_elem.assign(1, 0);
+    for (int v = 0; v < nv; ++v) {
+        const int s = vs_base[v];
+        ck.nrows.push_back(k.nrows[s]);
+        ck.sec_elem.push_back(ck.sec_elem.back() + k.nrows[s] * NC);
+        rb[v] = k.h_row_base[s];
+        r0[v] = k.h_row0[s];
+        ck.sec_tile0.push_back((int)ck.tile_sector.size());
+        ck.sec_ntiles.push_back(k.sec_ntiles[s]);
+        for (int t = 0; t < k.sec_ntiles[s]; ++t) {
+            ck.tile_sector.push_back(v);
+            ck.tile_row0.push_back(t * kBTile);
+        }
+    }
+    ck.n_tiles = (int)ck.tile_sector.size();
+    const int64_t tot_c = ck.sec_elem[nv];
+    const int n_prob_c = nv * NC;
+    auto up_i = [&](DevBuf<int>& d, const std::vector<int>& h) { d.alloc(h.size()); d.upload(h.data(), h.size(), st); };
+    auto up_l = [&](DevBuf<int64_t>& d, const std::vector<int64_t>& h) { d.alloc(h.size()); d.upload(h.data(), h.size(), st); };
+    up_i(ck.d_tile_sector, ck.tile_sector);
+    up_i(ck.d_tile_row0, ck.tile_row0);
+    up_i(ck.d_sec_tile0, ck.sec_tile0);
+    up_i(ck.d_sec_ntiles, ck.sec_ntiles);
+    up_l(ck.d_sec_elem, ck.sec_elem);
+    up_l(ck.d_nrows, ck.nrows);
+    up_l(ck.d_row_base, rb);
+    up_l(ck.d_row0, r0);
+    std::vector<int> ones(nv, 1);
+    up_i(ck.d_active, ones);
+    ck.d_ctr.alloc(2);
+    ck.d_ctr.zero(st);
+    ck.d_sec_ctr.alloc(nv);
+    ck.d_sec_ctr.zero(st);
+    DevBuf<int> d_vs_base, d_vs_set, d_real;
+    up_i(d_vs_base, vs_base);
+    up_i(d_vs_set, vs_set);
+    up_i(d_real, real);
+    // couplings of each slot
+    std::vector<double> hx(nsp_b), hz(nsp_b), cx(n_prob_c), cz(n_prob_c);
+    b->cxy.download(hx.data(), nsp_b, st);
+    b->cz.download(hz.data(), nsp_b, st);
+    QMB_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int pc = 0; pc < n_prob_c; ++pc) {
+        cx[pc] = hx[vs_set[pc]];
+        cz[pc] = hz[vs_set[pc]];
+    }
+    DevBuf<double> d_cx(n_prob_c), d_cz(n_prob_c);
+    d_cx.upload(cx.data(), n_prob_c, st);
+    d_cz.upload(cz.data(), n_prob_c, st);
+    BatchArgs ac = a_base;  // matrix arrays of the base kind
+    ac.n_sectors = nv;
+    ac.nsp = NC;
+    ac.tile_sector = ck.d_tile_sector.p;
+    ac.tile_row0 = ck.d_tile_row0.p;
+    ac.sec_elem = ck.d_sec_elem.p;
+    ac.sec_nrows = ck.d_nrows.p;
+    ac.row_base = ck.d_row_base.p;
+    ac.row0 = ck.d_row0.p;
+    ac.cxy = d_cx.p;
+    ac.cz = d_cz.p;
+    ac.c_stride = NC;
+    ac.active = ck.d_active.p;
+    // recurrence state: w_j, v_{j-1}, alpha/beta history, test state
+    const int64_t tot_b = k.sec_elem[k.n_sectors];
+    DevBuf<V> wc(2 * (size_t)tot_c), vc(2 * (size_t)tot_c);
+    k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
+                                                 wbuf + (int64_t)(j & 1) * tot_b, wc.p + (int64_t)(j & 1) * tot_c);
+    k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
+                                                 vring + (int64_t)((j + 1) & 1) * tot_b,
+                                                 vc.p + (int64_t)((j + 1) & 1) * tot_c);
+    DevBuf<double> alpha((size_t)(cap + 1) * n_prob_c), beta((size_t)(cap + 2) * n_prob_c),
+        partials((size_t)ck.n_tiles * NC), theta(n_prob_c), theta_prev(n_prob_c), gap(n_prob_c);
+    DevBuf<int> iter(1), msteps(n_prob_c), conv(n_prob_c), active_next(nv);
+    k_bgather_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(
+        n_prob_c, NC, nsp_b, lz_base.n_prob, j, d_vs_base.p, d_vs_set.p, d_real.p, lz_base.alpha, lz_base.beta,
+        theta_prev_b, msteps_b, gap_in, alpha.p, beta.p, theta_prev.p, msteps.p, gap.p, conv.p);
+    iter.upload(&j, 1, st);
+    check_launch("compaction");
+    BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob_c, ck.d_sec_ctr.p, ck.d_sec_tile0.p, ck.d_sec_ntiles.p};
+    auto step = [&](cudaStream_t ss) {
+        bhv_any<V>(ac, ck, wc.p, wc.p, vc.p, 2, lz, nullptr, nullptr, 1, ss);
+        bupdate_any<V>(ac, ck, wc.p, vc.p, 2, lz, ss);
+        k_badvance<<<1, 32, 0, ss>>>(lz);
+    };
+    int done = j;
+    {
+        DevBuf<int> d_w(nv);
+        d_w.upload(n_real.data(), nv, st);
+        LoopOut lo = device_loop(step, ac, lz, NC, stall, res_tol, e_tol, gap_in ? gap.p : nullptr, nullptr, theta.p,
+                                 theta_prev.p, msteps.p, conv.p, ck.d_active.p, active_next.p, ck.d_nrows.p, d_w.p,
+                                 nv, std::max(1, check), j, cap, 0.0, st);
+        done = lo.done;
+        products += lo.products;
+        n_hv += done - j;
+        if (trace_on())
+            std::fprintf(stderr, "[qmb batch] compacted %s loop: %d virtual sectors, steps %d..%d, stop reason %d\n",
+                         f64 ? "fp64" : "fp32", nv, j, done, lo.reason);
+        if (lo.reason != 1 && done < cap) {
+            std::vector<int> act(nv);
+            ck.d_active.download(act.data(), nv, st);
+            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+            double w = 0;
+            for (int v = 0; v < nv; ++v) w += (double)act[v] * n_real[v];
+            const int rem = cap - done;
+            for (int t = 0; t < rem; ++t) step(st);
+            products += rem * w;
+            done += rem;
+            n_hv += rem;
+            QMB_CUDA_TRY(cudaMemsetAsync(active_next.p, 0, sizeof(int) * nv, st));
+            launch_check(ac, lz, NC, stall, res_tol, e_tol, gap_in ? gap.p : nullptr, nullptr, theta.p,
+                         theta_prev.p, msteps.p, conv.p, active_next.p, done, st);
+            check_launch("compacted last steps");
+        }
+    }
+    k_bscatter_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(n_prob_c, NC, nsp_b, d_vs_base.p, d_vs_set.p,
+                                                            d_real.p, theta.p, msteps.p, conv.p, theta_b,
+                                                            msteps_b, conv_b);
+    check_launch("compaction results");
+    QMB_CUDA_TRY(cudaStreamSynchronize(st));
+    return done;
+}
+
 // Batched Lanczos phase over one kind with vectors V (and matrix values of
 // the same precision).  start: 0 splitmix (seed), 2 copy of psi_in (FP64).
 template <class V>
@@ -848,6 +1355,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
                          uint64_t seed, const void* psi_in, void* psi_out, int store_slots, int& n_hv,
                          cudaStream_t st, const int* init_active = nullptr) {
     BPhase out;
+    const auto t_begin = std::chrono::steady_clock::now();
     const int64_t tot = k.sec_elem[k.n_sectors];
     const int n_prob = k.n_sectors * b->nsp;
     int64_t minrows = INT64_MAX;
@@ -900,53 +1408,61 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
         bupdate_any<V>(a, k, wbuf.p, vring.p, K, lz, ss);
         k_badvance<<<1, 32, 0, ss>>>(lz);
     };
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    QMB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    step(st);
-    if (cudaStreamEndCapture(st, &graph) == cudaSuccess) {
-        if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) exec = nullptr;
-    }
-    cudaGetLastError();
     int done = 0;
-    std::vector<int> act(k.n_sectors);
-    std::vector<int> act_prev(k.n_sectors, 1);
-    if (init_active) {
-        QMB_CUDA_TRY(cudaMemcpyAsync(act_prev.data(), init_active, sizeof(int) * k.n_sectors,
-                                     cudaMemcpyDeviceToHost, st));
+    if (trace_on()) {
         QMB_CUDA_TRY(cudaStreamSynchronize(st));
+        std::fprintf(stderr, "[qmb batch] %s setup: %.2f ms\n", f64 ? "fp64" : "fp32",
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count());
     }
-    while (done < cap) {
-        int todo = std::min(std::max(1, check), cap - done);
-        for (int t = 0; t < todo; ++t) {
-            if (exec) QMB_CUDA_TRY(cudaGraphLaunch(exec, st));
-            else step(st);
-        }
-        check_launch("batch step");
-        {
+    {
+        std::vector<int> wts(k.n_sectors, b->n_sets);
+        DevBuf<int> d_w(k.n_sectors);
+        d_w.upload(wts.data(), k.n_sectors, st);
+        const bool can_compact = !psi_out && K == 2;
+        LoopOut lo = device_loop(step, a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p,
+                                 theta_prev.p, msteps.p, conv.p, k.d_active.p, active_next.p, k.d_nrows.p, d_w.p,
+                                 k.n_sectors, std::max(1, check), 0, cap, can_compact ? 0.4 : 0.0, st);
+        done = lo.done;
+        out.products += lo.products;
+        n_hv += done;
+        if (trace_on())
+            std::fprintf(stderr, "[qmb batch] %s loop: %d steps, stop reason %d, %.2f ms to here\n",
+                         f64 ? "fp64" : "fp32", done, lo.reason,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count());
+        if (lo.reason == 3) {
+            std::vector<int> hc(n_prob);
+            conv.download(hc.data(), n_prob, st);
+            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+            const int j0 = done;
+            done = run_compacted<V>(b, k, f64, a, lz, wbuf.p, vring.p, done, cap, stall, res_tol, e_tol, gap_in,
+                                    check, hc, theta.p, theta_prev.p, msteps.p, conv.p, out.products, n_hv, st);
+            (void)j0;
+        } else if (lo.reason != 1 && done < cap) {
+            // the last steps (fewer than a block) with one test at the end
+            std::vector<int> act(k.n_sectors);
+            k.d_active.download(act.data(), k.n_sectors, st);
+            QMB_CUDA_TRY(cudaStreamSynchronize(st));
             int na = 0;
-            for (int v : act_prev) na += v;
-            out.products += (double)todo * na * b->n_sets;
+            for (int v : act) na += v;
+            const int rem = cap - done;
+            for (int t = 0; t < rem; ++t) step(st);
+            out.products += (double)rem * na * b->n_sets;
+            done += rem;
+            n_hv += rem;
+            QMB_CUDA_TRY(cudaMemsetAsync(active_next.p, 0, sizeof(int) * k.n_sectors, st));
+            launch_check(a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p, theta_prev.p,
+                         msteps.p, conv.p, active_next.p, done, st);
+            QMB_CUDA_TRY(cudaMemcpyAsync(k.d_active.p, active_next.p, sizeof(int) * k.n_sectors,
+                                         cudaMemcpyDeviceToDevice, st));
+            check_launch("batch last steps");
         }
-        done += todo;
-        n_hv += todo;
-        QMB_CUDA_TRY(cudaMemsetAsync(active_next.p, 0, sizeof(int) * k.n_sectors, st));
-        k_bcheck<<<rg, rb, 0, st>>>(a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p,
-                                    theta_prev.p, msteps.p, conv.p, active_next.p, Ls.p, Ds.p, ritz.p);
-        QMB_CUDA_TRY(cudaMemcpyAsync(k.d_active.p, active_next.p, sizeof(int) * k.n_sectors,
-                                     cudaMemcpyDeviceToDevice, st));
-        active_next.download(act.data(), k.n_sectors, st);
-        QMB_CUDA_TRY(cudaStreamSynchronize(st));
-        bool any = false;
-        for (int v : act) any |= v != 0;
-        act_prev = act;
-        if (!any) break;
     }
     out.steps = done;
     if (trace_on()) {
         QMB_CUDA_TRY(cudaStreamSynchronize(st));
-        std::fprintf(stderr, "[qmb batch] phase %s: %d steps, ring %d, start %d\n", f64 ? "fp64" : "fp32",
-                     done, K, start);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+        std::fprintf(stderr, "[qmb batch] phase %s: %d steps, ring %d, start %d, %.2f ms to here\n",
+                     f64 ? "fp64" : "fp32", done, K, start, ms);
     }
     // Ritz vectors (FP64) for the next phase or the caller
     if (psi_out) {
@@ -981,8 +1497,6 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     msteps.download(out.msteps.data(), n_prob, st);
     conv.download(out.conv.data(), n_prob, st);
     QMB_CUDA_TRY(cudaStreamSynchronize(st));
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
     return out;
 }
 
@@ -1131,6 +1645,8 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             up_l(K.d_row_ptr, row_ptr);
             up_l(K.d_row_base, row_base);
             up_l(K.d_row0, row0);
+            K.h_row_base = row_base;
+            K.h_row0 = row0;
             K.d_col.alloc(std::max<size_t>(1, col.size()));
             if (!col.empty()) K.d_col.upload(col.data(), col.size());
             // values in the sector kind's scalar types

@@ -84,3 +84,32 @@ def test_batch_dense_oracle_and_hv():
         for i in (0, 5):
             want = J[i] * (M @ xv[:, i]) + J[i] * D[i] * (Dz @ xv[:, i])
             np.testing.assert_allclose(yv[:, i], want, atol=1e-11 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("mode", [A.MODE_FP64, A.MODE_MIXED, A.MODE_FP32])
+def test_batch_many_sets_dense_oracle(mode):
+    """200 coupling sets x 12 sectors: convergence spreads over many steps,
+    so the unconverged tail continues in a compacted sub-batch.  Every
+    energy is checked against dense diagonalisation of its sector matrix."""
+    L, n_sets = 12, 200
+    secs, perm, ch = _sectors(L)
+    bonds = q.chain_bonds(L)
+    b = q.Batch(secs, q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"), n_sets)
+    rng = np.random.default_rng(7)
+    D = rng.uniform(0, 2, n_sets)
+    J = rng.uniform(0.5, 1.5, n_sets)
+    E, summ = b.solve(J, J * D, mode=mode, max_iter=300, tol=1e-12)
+    g = oracle_group(perm, ch)
+    sec = O.build_sector(g, L // 2)
+    txy, tz = q.xxz_terms(bonds, 1.0, 0.0), q.xxz_terms(bonds, 0.0, 1.0)
+    tol = 1e-5 if mode == A.MODE_FP32 else 1e-10
+    for a in range(L):
+        rows = O.active_rows(sec, a)
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(txy), a, 2 * txy.n_terms + 1)
+        Axy = O.ell_to_csr(ind, val, tr, rows).toarray()
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(tz), a, 2 * tz.n_terms + 1)
+        Dz = O.ell_to_csr(ind, val, tr, rows).toarray()
+        H = J[:, None, None] * Axy[None] + (J * D)[:, None, None] * Dz[None]
+        e = np.linalg.eigvalsh(H)[:, 0]
+        err = np.abs(E[:, a] - e) / np.maximum(np.abs(e), 1.0)
+        assert err.max() <= tol, (a, err.max(), int(err.argmax()))

@@ -164,7 +164,7 @@ def run_batched(args, torch, q, rank, world):
     for _ in range(args.warmup):
         solve(A.MODE_MIXED)
     torch.cuda.synchronize()
-    dev_ms, hv_count = [], []
+    dev_ms, hv_count, launches = [], [], 0
     with Clocks(torch.cuda.current_device()) as clk:
         for _ in range(args.steps):
             flush_l2(torch, flush)
@@ -172,6 +172,7 @@ def run_batched(args, torch, q, rank, world):
             E_mix, r = solve(A.MODE_MIXED)
             dev_ms.append(r.ms_total)
             hv_count.append(r.n_products)
+            launches += int(r.n_launches)
     clocks = clk.summary()
     # FP64 reference solve of the same problems, |dE0| of the mixed result
     if args.no_compare:
@@ -229,7 +230,8 @@ def run_batched(args, torch, q, rank, world):
                 extra=extra, clocks=clocks, e2e_s=e2e_s,
                 e2e_value=float(np.mean(hv_count)) / e2e_s,
                 h2d=2 * n_sets * 8, d2h=n_sets * L * 8, roof_bytes=roof_bytes, roof_ms=hv32_ms,
-                launches=int(r.n_hv) * 3, kernel="k_bhv<float2,2,*,*> (batched H*v, FP32 complex)",
+                launches=launches,
+                kernel="k_bhv (batched H*v, FP32; one launch for the complex sectors, one for the real ones)",
                 dtype="f32+f64")
 
 
@@ -294,6 +296,19 @@ def cpu_reference_hv(seconds=10.0, threads=None):
                                 f"{count} H*v in {dt:.1f} s"
 
 
+def aggregate_ranks(torch, dist, ms, e2e_s, units, device):
+    """Whole-job figures of a weak-scaling run: every rank solves its own
+    coupling sets, the step time is the maximum over ranks and the work is
+    the sum over ranks.  Returns (max ms, max end-to-end s, total units)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return ms, e2e_s, units
+    t = torch.tensor([ms, e2e_s], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    u = torch.tensor([units], device=device, dtype=torch.float64)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), float(u[0])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -349,14 +364,7 @@ def main():
     if dist:
         dist.barrier()
     res = run_batched(args, torch, q, rank, world)
-    ms = res["ms"]
-    if dist:
-        t = torch.tensor([ms, res["e2e_s"]], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(t[0]), float(t[1])
-    else:
-        e2e_s = res["e2e_s"]
-    total_units = res["units_per_step"] * world
+    ms, e2e_s, total_units = aggregate_ranks(torch, dist, res["ms"], res["e2e_s"], res["units_per_step"], "cuda")
     value = total_units / (ms * 1e-3)
     peak, peak_kind = load_peaks()
     achieved = res["roof_bytes"] / (res["roof_ms"] * 1e-3) / 1e9

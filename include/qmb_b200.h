@@ -296,6 +296,8 @@ typedef struct {
     double ms_hv;        /* device time inside H*v kernels (-1: not measured) */
     double n_products;   /* H*v products of single problems computed (batches: active
                             sectors x coupling sets per step; single solves: n_hv) */
+    double n_launches;   /* kernels of this library executed by the call (launches
+                            plus kernel nodes run by its CUDA graphs) */
 } qmb_lanczos_result;
 
 QMB_API void qmb_lanczos_default_opts(qmb_lanczos_opts* o);

@@ -74,7 +74,7 @@ class LanczosResult(C.Structure):
     _fields_ = [("E0", C.c_double), ("E0_low", C.c_double), ("residual", C.c_double),
                 ("residual_ref", C.c_double), ("iters", C.c_int), ("iters_low", C.c_int),
                 ("n_hv", C.c_int), ("converged", C.c_int), ("ms_total", C.c_double),
-                ("ms_hv", C.c_double), ("n_products", C.c_double)]
+                ("ms_hv", C.c_double), ("n_products", C.c_double), ("n_launches", C.c_double)]
 
 
 class BatchDesc(C.Structure):

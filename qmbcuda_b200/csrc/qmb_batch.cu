@@ -30,6 +30,10 @@ namespace qmb {
 constexpr int kBThreads = 256;      // threads per block
 constexpr int kBTile = 32;          // rows per work item
 
+// Kernels of this file executed for the current batched call on this thread
+// (launches, plus kernel nodes run by the CUDA graphs).
+thread_local double g_kernels = 0;
+
 struct BatchArgs {
     int n_sectors;
     int nsp;                     // padded sets: 32, 64, 128 or 256
@@ -977,6 +981,7 @@ static void launch_bhv_v(const BatchArgs& a, BKind& k, const V* x, V* y, V* vrin
     const size_t smem = (size_t)a.max_tile_entries * (sizeof(V) + sizeof(uint32_t));
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_bhv<V, SPL, UNR, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    g_kernels += 1;
     k_bhv<V, SPL, UNR, MINB><<<std::min(g, k.n_tiles), kBThreads, smem, st>>>(
         a, k.n_tiles, k.d_ctr.p, x, y, vring, K, lz, ritz, psi, lanczos);
 }
@@ -1064,12 +1069,14 @@ template <class V>
 static void bupdate_any(const BatchArgs& a, const BKind& k, V* w, const V* vring, int K, BLz lz,
                         cudaStream_t st) {
     if (k.n_tiles == 0) return;
+    g_kernels += 1;
     k_bupdate<V><<<k.n_tiles, a.nsp, 0, st>>>(a, k.n_tiles, w, vring, K, lz);
 }
 
 template <class V>
 static void bnorm0_any(const BatchArgs& a, const BKind& k, const V* w, BLz lz, cudaStream_t st) {
     if (k.n_tiles == 0) return;
+    g_kernels += 1;
     k_bnorm0<V><<<k.n_tiles, a.nsp, 0, st>>>(a, k.n_tiles, w, lz);
 }
 
@@ -1113,6 +1120,7 @@ static void launch_check(const BatchArgs& a, const BLz& lz, int nsets, double st
     if (smem > (48u << 10))
         cudaFuncSetAttribute(k_bcheck, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int nblk = (lz.n_prob + wpb - 1) / wpb;
+    g_kernels += 1;
     k_bcheck<<<nblk, 32 * wpb, smem, st>>>(a, lz, nsets, stall, res_tol, e_tol, gap_in, gap_out, theta,
                                            theta_prev, msteps, conv, active_next, open_cnt);
 }
@@ -1166,14 +1174,18 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
     QMB_CUDA_TRY(cudaGraphAddNode(&node, g, nullptr, 0, &np));
     cudaGraph_t body = np.conditional.phGraph_out[0];
     QMB_CUDA_TRY(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const double kernels_before = g_kernels;  // capture records kernels; they run once per loop
     for (int t = 0; t < check; ++t) step(st);
     launch_check(a, lz, nsets, stall, res_tol, e_tol, gap_in, gap_out, theta, theta_prev, msteps, conv,
                  active_next, cap, st, open_cnt.p);
+    g_kernels += 1;
     k_bloop_ctl<<<1, 256, 0, st>>>(h, n_sectors, active, active_next, open_cnt.p, d_nrows, d_weight, a.nsp,
                                    check, cap, lz.iter, max_loops, compact_ratio, ctl.p);
     cudaGraph_t captured = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &captured);
     QMB_CUDA_TRY(ce);
+    const double body_kernels = g_kernels - kernels_before;
+    g_kernels = kernels_before;
     QMB_CUDA_TRY(cudaGraphInstantiate(&ex, g, 0));
     QMB_CUDA_TRY(cudaGraphLaunch(ex, st));
     LoopCtl hc;
@@ -1184,6 +1196,7 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
     out.done = it;
     out.reason = hc.reason;
     out.products = hc.products;
+    g_kernels += body_kernels * hc.loops;
     return out;
 }
 
@@ -1290,14 +1303,17 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     // recurrence state: w_j, v_{j-1}, alpha/beta history, test state
     const int64_t tot_b = k.sec_elem[k.n_sectors];
     DevBuf<V> wc(2 * (size_t)tot_c), vc(2 * (size_t)tot_c);
+    g_kernels += 1;
     k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
                                                  wbuf + (int64_t)(j & 1) * tot_b, wc.p + (int64_t)(j & 1) * tot_c);
+    g_kernels += 1;
     k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
                                                  vring + (int64_t)((j + 1) & 1) * tot_b,
                                                  vc.p + (int64_t)((j + 1) & 1) * tot_c);
     DevBuf<double> alpha((size_t)(cap + 1) * n_prob_c), beta((size_t)(cap + 2) * n_prob_c),
         partials((size_t)ck.n_tiles * NC), theta(n_prob_c), theta_prev(n_prob_c), gap(n_prob_c);
     DevBuf<int> iter(1), msteps(n_prob_c), conv(n_prob_c), active_next(nv);
+    g_kernels += 1;
     k_bgather_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(
         n_prob_c, NC, nsp_b, lz_base.n_prob, j, d_vs_base.p, d_vs_set.p, d_real.p, lz_base.alpha, lz_base.beta,
         theta_prev_b, msteps_b, gap_in, alpha.p, beta.p, theta_prev.p, msteps.p, gap.p, conv.p);
@@ -1307,6 +1323,7 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     auto step = [&](cudaStream_t ss) {
         bhv_any<V>(ac, ck, wc.p, wc.p, vc.p, 2, lz, nullptr, nullptr, 1, ss);
         bupdate_any<V>(ac, ck, wc.p, vc.p, 2, lz, ss);
+        g_kernels += 1;
         k_badvance<<<1, 32, 0, ss>>>(lz);
     };
     int done = j;
@@ -1339,6 +1356,7 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
             check_launch("compacted last steps");
         }
     }
+    g_kernels += 1;
     k_bscatter_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(n_prob_c, NC, nsp_b, d_vs_base.p, d_vs_set.p,
                                                             d_real.p, theta.p, msteps.p, conv.p, theta_b,
                                                             msteps_b, conv_b);
@@ -1399,13 +1417,16 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob, k.d_sec_ctr.p, k.d_sec_tile0.p, k.d_sec_ntiles.p};
     const int rb = 256, rg = (n_prob + rb - 1) / rb;
     tuned_variant<V>(a, k, f64, st);
+    g_kernels += 1;
     k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
     bnorm0_any<V>(a, k, wbuf.p, lz, st);
+    g_kernels += 1;
     k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
     check_launch("batch start");
     auto step = [&](cudaStream_t ss) {
         bhv_any<V>(a, k, wbuf.p, wbuf.p, vring.p, K, lz, nullptr, nullptr, 1, ss);
         bupdate_any<V>(a, k, wbuf.p, vring.p, K, lz, ss);
+        g_kernels += 1;
         k_badvance<<<1, 32, 0, ss>>>(lz);
     };
     int done = 0;
@@ -1467,22 +1488,27 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     // Ritz vectors (FP64) for the next phase or the caller
     if (psi_out) {
         DevBuf<double> xs((size_t)(cap + 1) * n_prob);
+        g_kernels += 1;
         k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p, gap_out);
         if (K > 2 && done < K) {
+            g_kernels += 1;
             k_bpsi<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, vring.p, K, msteps.p, ritz.p, n_prob,
                                                           psi_out);
         } else {
             QMB_CUDA_TRY(cudaMemsetAsync(psi_out, 0, (Sc<V>::cplx ? 16 : 8) * tot, st));
             std::vector<int> all(k.n_sectors, 1);
             k.d_active.upload(all.data(), k.n_sectors, st);
+            g_kernels += 1;
             k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
             bnorm0_any<V>(a, k, wbuf.p, lz, st);
+            g_kernels += 1;
             k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
             // regeneration runs every problem to the longest m; coefficients
             // beyond a problem's own m are zero (k_britz wrote m entries)
             for (int j = 0; j < done; ++j) {
                 bhv_any<V>(a, k, wbuf.p, wbuf.p, vring.p, K, lz, ritz.p, psi_out, 1, st);
                 bupdate_any<V>(a, k, wbuf.p, vring.p, K, lz, st);
+                g_kernels += 1;
                 k_badvance<<<1, 32, 0, st>>>(lz);
                 ++n_hv;
                 out.products += (double)k.n_sectors * b->n_sets;
@@ -1807,6 +1833,7 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
         b->cz.upload(hz.data(), b->nsp, st);
         const int check = o.check_every > 0 ? o.check_every : 10;
         const double tol64 = o.tol > 0 ? o.tol : 1e-12;
+        g_kernels = 0;
         int n_hv = 0, it_low = 0, it_tot = 0;
         double products = 0;
         bool all_conv = true;
@@ -1864,18 +1891,25 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                         if (kd) {
                             tuned_variant<double2>(a, k, true, st);
                             bhv_any<double2>(a, k, (const double2*)psi.p, (double2*)hy.p, nullptr, 1, lz0, nullptr, nullptr, 0, st);
+                            g_kernels += 1;
                             k_bdot<double2><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double2*)psi.p, (const double2*)hy.p, nullptr, part.p);
                         } else {
                             tuned_variant<double>(a, k, true, st);
                             bhv_any<double>(a, k, (const double*)psi.p, (double*)hy.p, nullptr, 1, lz0, nullptr, nullptr, 0, st);
+                            g_kernels += 1;
                             k_bdot<double><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double*)psi.p, (const double*)hy.p, nullptr, part.p);
                         }
+                        g_kernels += 1;
                         k_bsum<<<rg2, rb2, 0, st>>>(a, k.n_tiles, k.d_sec_tile0.p, k.d_sec_ntiles.p, part.p, 2, n_prob, sums.p);
+                        g_kernels += 1;
                         k_brq_energy<<<rg2, rb2, 0, st>>>(n_prob, sums.p, Eq.p);
+                        g_kernels += 1;
                         if (kd) k_bdot<double2><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double2*)psi.p, (const double2*)hy.p, Eq.p, part.p);
                         else k_bdot<double><<<k.n_tiles, b->nsp, 0, st>>>(a, k.n_tiles, (const double*)psi.p, (const double*)hy.p, Eq.p, part.p);
+                        g_kernels += 1;
                         k_bsum<<<rg2, rb2, 0, st>>>(a, k.n_tiles, k.d_sec_tile0.p, k.d_sec_ntiles.p, part.p, 1, n_prob, r2.p);
                         act_d.zero(st);
+                        g_kernels += 1;
                         k_brq_accept<<<rg2, rb2, 0, st>>>(a, n_prob, b->n_sets, Eq.p, r2.p, sums.p + n_prob, gapb.p, tol64, ok.p, act_d.p);
                         check_launch("rq check");
                         Eq.download(e_rq.data(), n_prob, st);
@@ -1953,6 +1987,7 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
             summary->iters_low = it_low;
             summary->n_hv = n_hv;
             summary->n_products = products;
+            summary->n_launches = g_kernels;
             summary->converged = all_conv ? 1 : 0;
             summary->E0 = *std::min_element(result.begin(), result.end());
             summary->E0_low = o.mode == QMB_MODE_FP64 ? summary->E0 : *std::min_element(low.begin(), low.end());

@@ -28,6 +28,9 @@ namespace qmb {
 
 constexpr int kLzBlock = 256;
 
+// Kernels executed for the current qmb_lanczos call on this thread.
+thread_local double g_lz_kernels = 0;
+
 struct LzDev {
     double* alpha;      // [cap]
     double* beta;       // [cap + 1]
@@ -345,6 +348,7 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
     const int nb = st.nb;
     QMB_REQUIRE(po.reorth == 0 || store, QMB_ERR_INVALID, "reorthogonalisation needs the stored basis");
 
+    g_lz_kernels += 1;
     k_lz_start<V, P><<<nb, kLzBlock, 0, s>>>(n, start_mode, seed, from, wbuf.p, st.d);
     check_launch("k_lz_start");
 
@@ -389,6 +393,7 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
             if (exec) QMB_CUDA_TRY(cudaGraphLaunch(exec, s));
             else step(s);
         }
+        g_lz_kernels += (double)todo * (2 + 2 * po.reorth);
         check_launch("lanczos step");
         done += todo;
         out.n_hv += todo;
@@ -482,6 +487,7 @@ void ritz_vector(const Op& op, size_t op_smem, const PhaseOut& ph, int start_mod
     DevBuf<double> ritz(ph.m);
     ritz.upload(for_restart ? ph.s_start.data() : ph.s.data(), ph.m, s);
     if (stored) {
+        g_lz_kernels += 1;
         k_ritz<V, P><<<grid_for(n, 256), 256, 0, s>>>(n, vring.p, ph.m, ritz.p, psi);
         check_launch("k_ritz");
         QMB_CUDA_TRY(cudaStreamSynchronize(s));
@@ -490,6 +496,7 @@ void ritz_vector(const Op& op, size_t op_smem, const PhaseOut& ph, int start_mod
     // regenerate v_0..v_{m-1} with the same start; kernels are deterministic
     QMB_CUDA_TRY(cudaMemsetAsync(psi, 0, sizeof(P) * n, s));
     const int nb = st.nb;
+    g_lz_kernels += 2 * ph.m;  // start, m products, m - 1 updates
     k_lz_start<V, P><<<nb, kLzBlock, 0, s>>>(n, start_mode, seed, from, wbuf.p, st.d);
     for (int j = 0; j < ph.m; ++j) {
         k_lz_hv<Op, V, P><<<nb, kLzBlock, op_smem, s>>>(op, wbuf.p, vring.p, K, st.d, ritz.p, psi);
@@ -504,6 +511,7 @@ template <class Op, class P>
 double residual_norm(const Op& op, size_t op_smem, const P* psi, double theta, LzState& st,
                      cudaStream_t s, double* psi_norm2) {
     set_group_smem_attr((const void*)k_residual<Op, P>, op_smem);
+    g_lz_kernels += 1;
     k_residual<Op, P><<<st.nb, kLzBlock, op_smem, s>>>(op, psi, theta, st.d);
     check_launch("k_residual");
     double h[2];
@@ -535,6 +543,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     const int64_t n = h->n;
     std::memset(res, 0, sizeof(*res));
     res->ms_hv = -1;
+    g_lz_kernels = 0;
     LzState st;
     PhaseOpts po;
     po.max_iter = o.max_iter;
@@ -648,6 +657,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     res->iters = iters;
     res->n_hv = n_hv;
     res->n_products = n_hv;
+    res->n_launches = g_lz_kernels;
     res->converged = conv ? 1 : 0;
     if (o.mode == QMB_MODE_FP64) res->E0_low = theta;
     if (coeffs) {

@@ -175,9 +175,13 @@ def run_batched(args, torch, q, rank, world):
             launches += int(r.n_launches)
     clocks = clk.summary()
     # FP64 reference solve of the same problems, |dE0| of the mixed result
+    # (after one warm-up FP64 solve, which sizes the FP64 workspace)
     if args.no_compare:
         E64, r64 = E_mix, r
     else:
+        solve(A.MODE_FP64)
+        flush_l2(torch, flush)
+        torch.cuda.synchronize()
         E64, r64 = solve(A.MODE_FP64)
     rel = np.abs(E_mix - E64) / np.maximum(np.abs(E64), 1e-300)
     # per-kernel H*v times

@@ -34,6 +34,42 @@ constexpr int kBTile = 32;          // rows per work item
 // (launches, plus kernel nodes run by the CUDA graphs).
 thread_local double g_kernels = 0;
 
+// Non-owning view of device memory with DevBuf's helpers.
+template <class T>
+struct Buf {
+    T* p = nullptr;
+    size_t n = 0;
+    void zero(cudaStream_t st = 0) { QMB_CUDA_TRY(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
+    void upload(const T* h, size_t count, cudaStream_t st = 0) {
+        QMB_CUDA_TRY(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
+    }
+    void download(T* h, size_t count, cudaStream_t st = 0) const {
+        QMB_CUDA_TRY(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, st));
+    }
+};
+
+// Temporaries of a batched solve, kept for the next solve: ws_take() hands
+// out the pool's buffers in call order and grows one only when a request is
+// larger than it, so a solve that repeats an earlier one allocates nothing
+// (no cudaMalloc / cudaFree, whose device-wide synchronisation and driver
+// latency would otherwise sit inside the solve).
+struct WsPool {
+    std::vector<std::unique_ptr<DevBuf<unsigned char>>> bufs;
+    size_t next = 0;
+};
+thread_local WsPool* g_ws = nullptr;  // pool of the solve running on this thread
+
+template <class T>
+static Buf<T> ws_take(size_t count) {
+    if (count == 0) count = 1;
+    QMB_REQUIRE(g_ws, QMB_ERR_INVALID, "internal: workspace taken outside a batched solve");
+    WsPool& w = *g_ws;
+    if (w.next == w.bufs.size()) w.bufs.emplace_back(new DevBuf<unsigned char>());
+    DevBuf<unsigned char>& d = *w.bufs[w.next++];
+    if (d.n < count * sizeof(T)) d.alloc(count * sizeof(T));
+    return Buf<T>{reinterpret_cast<T*>(d.p), count};
+}
+
 struct BatchArgs {
     int n_sectors;
     int nsp;                     // padded sets: 32, 64, 128 or 256
@@ -385,7 +421,7 @@ __global__ void k_brq_accept(BatchArgs a, int n_prob, int nsets, const double* _
 
 template <class V>
 __global__ void k_bstart(BatchArgs a, int64_t tot, int mode, uint64_t seed, const void* from,
-                         V* __restrict__ w0) {
+                         V* __restrict__ w0, const int64_t* __restrict__ order) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot;
          i += (int64_t)gridDim.x * blockDim.x) {
         V v;
@@ -400,8 +436,21 @@ __global__ void k_bstart(BatchArgs a, int64_t tot, int mode, uint64_t seed, cons
                 z ^= z >> 31;
                 return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
             };
-            if constexpr (Sc<V>::cplx) v = Sc<V>::from(make_double2(u(2 * i), u(2 * i + 1)));
-            else v = Sc<V>::from(make_double2(u(i), 0.0));
+            // the random value belongs to the (sector, original row, set)
+            // element, whatever the row order of the layout
+            int64_t c = i;
+            if (order) {
+                int lo = 0, hi = a.n_sectors - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (a.sec_elem[mid] <= i) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int64_t loc = i - a.sec_elem[lo];
+                c = a.sec_elem[lo] + order[a.row0[lo] + loc / a.nsp] * a.nsp + loc % a.nsp;
+            }
+            if constexpr (Sc<V>::cplx) v = Sc<V>::from(make_double2(u(2 * c), u(2 * c + 1)));
+            else v = Sc<V>::from(make_double2(u(c), 0.0));
         }
         w0[i] = v;
     }
@@ -916,9 +965,17 @@ struct BKind {
     DevBuf<unsigned> d_sec_ctr;  // per-sector finished tiles
     int variant[2] = {-1, -1};    // tuned k_bhv variant per precision (FP32, FP64)
     DevBuf<unsigned char> ws_ring, ws_w;  // Lanczos workspace kept between solves
+    std::unique_ptr<BKind> compact;        // descriptor of the last compacted sub-batch
     float tune_ms[2][4] = {};
     DevBuf<int64_t> d_sec_elem, d_nrows, d_row_ptr, d_row_base, d_row0;
     std::vector<int64_t> h_row_base, h_row0;  // per sector, as on the device
+    // the same matrices with each sector's rows in reverse Cuthill-McKee order
+    // (same row_base / row0 offsets), used by the solver; order maps an RCM
+    // row to its original row
+    DevBuf<int64_t> d_rcm_row_ptr, d_order;
+    DevBuf<uint32_t> d_rcm_col;
+    DevBuf<unsigned char> rval64, rval32, rdxy64, rdxy32, rdz64, rdz32;
+    std::vector<int64_t> bandwidth;  // per sector, max |col - row| in RCM order
     DevBuf<uint32_t> d_col;
     DevBuf<unsigned char> val64, val32, dxy64, dxy32, dz64, dz32;
     int64_t nnz = 0, rows = 0;
@@ -930,13 +987,14 @@ struct qmb_batch_s {
     int device = 0;
     int n_sectors = 0, n_sets = 0, nsp = 0, spl = 8, n_groups = 1;
     BKind kind[2];  // 0 real, 1 complex
+    qmb::WsPool ws;  // temporaries of the solves, reused from one solve to the next
     std::vector<int> sector_kind, sector_pos;
     DevBuf<double> cxy, cz;
 };
 
 namespace qmb {
 
-static BatchArgs make_args(const qmb_batch_s* b, const BKind& k) {
+static BatchArgs make_args(const qmb_batch_s* b, const BKind& k, bool rcm = false) {
     BatchArgs a;
     a.n_sectors = k.n_sectors;
     a.nsp = b->nsp;
@@ -945,10 +1003,10 @@ static BatchArgs make_args(const qmb_batch_s* b, const BKind& k) {
     a.tile_row0 = k.d_tile_row0.p;
     a.sec_elem = k.d_sec_elem.p;
     a.sec_nrows = k.d_nrows.p;
-    a.row_ptr = k.d_row_ptr.p;
+    a.row_ptr = rcm ? k.d_rcm_row_ptr.p : k.d_row_ptr.p;
     a.row_base = k.d_row_base.p;
     a.row0 = k.d_row0.p;
-    a.col = k.d_col.p;
+    a.col = rcm ? k.d_rcm_col.p : k.d_col.p;
     a.val = nullptr;
     a.dxy = nullptr;
     a.dz = nullptr;
@@ -1144,8 +1202,8 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
                            int cap, double compact_ratio, cudaStream_t st) {
     LoopOut out{j0, 2, 0.0};
     if (j0 + check > cap) return out;
-    DevBuf<LoopCtl> ctl(1);
-    DevBuf<int> open_cnt(n_sectors);
+    Buf<LoopCtl> ctl = ws_take<LoopCtl>(1);
+    Buf<int> open_cnt = ws_take<int>(n_sectors);
     ctl.zero(st);
     open_cnt.zero(st);
     QMB_CUDA_TRY(cudaMemsetAsync(active_next, 0, sizeof(int) * n_sectors, st));
@@ -1232,7 +1290,14 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     }
     const int nv = (int)vs_base.size();
     if (nv == 0) return j;
-    BKind ck;
+    // the compacted layout's descriptor is kept on the kind and refilled
+    if (!k.compact) k.compact = std::make_unique<BKind>();
+    BKind& ck = *k.compact;
+    ck.nrows.clear();
+    ck.sec_tile0.clear();
+    ck.sec_ntiles.clear();
+    ck.tile_sector.clear();
+    ck.tile_row0.clear();
     ck.n_sectors = nv;
     ck.variant[0] = k.variant[0];
     ck.variant[1] = k.variant[1];
@@ -1255,8 +1320,14 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     ck.n_tiles = (int)ck.tile_sector.size();
     const int64_t tot_c = ck.sec_elem[nv];
     const int n_prob_c = nv * NC;
-    auto up_i = [&](DevBuf<int>& d, const std::vector<int>& h) { d.alloc(h.size()); d.upload(h.data(), h.size(), st); };
-    auto up_l = [&](DevBuf<int64_t>& d, const std::vector<int64_t>& h) { d.alloc(h.size()); d.upload(h.data(), h.size(), st); };
+    auto up_i = [&](DevBuf<int>& d, const std::vector<int>& h) {
+        if (d.n < h.size()) d.alloc(h.size());
+        d.upload(h.data(), h.size(), st);
+    };
+    auto up_l = [&](DevBuf<int64_t>& d, const std::vector<int64_t>& h) {
+        if (d.n < h.size()) d.alloc(h.size());
+        d.upload(h.data(), h.size(), st);
+    };
     up_i(ck.d_tile_sector, ck.tile_sector);
     up_i(ck.d_tile_row0, ck.tile_row0);
     up_i(ck.d_sec_tile0, ck.sec_tile0);
@@ -1267,14 +1338,15 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     up_l(ck.d_row0, r0);
     std::vector<int> ones(nv, 1);
     up_i(ck.d_active, ones);
-    ck.d_ctr.alloc(2);
+    if (ck.d_ctr.n < 2) ck.d_ctr.alloc(2);
     ck.d_ctr.zero(st);
-    ck.d_sec_ctr.alloc(nv);
+    if (ck.d_sec_ctr.n < (size_t)nv) ck.d_sec_ctr.alloc(nv);
     ck.d_sec_ctr.zero(st);
-    DevBuf<int> d_vs_base, d_vs_set, d_real;
-    up_i(d_vs_base, vs_base);
-    up_i(d_vs_set, vs_set);
-    up_i(d_real, real);
+    Buf<int> d_vs_base = ws_take<int>(vs_base.size()), d_vs_set = ws_take<int>(vs_set.size()),
+             d_real = ws_take<int>(real.size());
+    d_vs_base.upload(vs_base.data(), vs_base.size(), st);
+    d_vs_set.upload(vs_set.data(), vs_set.size(), st);
+    d_real.upload(real.data(), real.size(), st);
     // couplings of each slot
     std::vector<double> hx(nsp_b), hz(nsp_b), cx(n_prob_c), cz(n_prob_c);
     b->cxy.download(hx.data(), nsp_b, st);
@@ -1284,7 +1356,8 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
         cx[pc] = hx[vs_set[pc]];
         cz[pc] = hz[vs_set[pc]];
     }
-    DevBuf<double> d_cx(n_prob_c), d_cz(n_prob_c);
+    Buf<double> d_cx = ws_take<double>(n_prob_c),
+        d_cz = ws_take<double>(n_prob_c);
     d_cx.upload(cx.data(), n_prob_c, st);
     d_cz.upload(cz.data(), n_prob_c, st);
     BatchArgs ac = a_base;  // matrix arrays of the base kind
@@ -1302,7 +1375,8 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     ac.active = ck.d_active.p;
     // recurrence state: w_j, v_{j-1}, alpha/beta history, test state
     const int64_t tot_b = k.sec_elem[k.n_sectors];
-    DevBuf<V> wc(2 * (size_t)tot_c), vc(2 * (size_t)tot_c);
+    Buf<V> wc = ws_take<V>(2 * (size_t)tot_c),
+        vc = ws_take<V>(2 * (size_t)tot_c);
     g_kernels += 1;
     k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
                                                  wbuf + (int64_t)(j & 1) * tot_b, wc.p + (int64_t)(j & 1) * tot_c);
@@ -1310,9 +1384,16 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
                                                  vring + (int64_t)((j + 1) & 1) * tot_b,
                                                  vc.p + (int64_t)((j + 1) & 1) * tot_c);
-    DevBuf<double> alpha((size_t)(cap + 1) * n_prob_c), beta((size_t)(cap + 2) * n_prob_c),
-        partials((size_t)ck.n_tiles * NC), theta(n_prob_c), theta_prev(n_prob_c), gap(n_prob_c);
-    DevBuf<int> iter(1), msteps(n_prob_c), conv(n_prob_c), active_next(nv);
+    Buf<double> alpha = ws_take<double>((size_t)(cap + 1) * n_prob_c),
+        beta = ws_take<double>((size_t)(cap + 2) * n_prob_c),
+        partials = ws_take<double>((size_t)ck.n_tiles * NC),
+        theta = ws_take<double>(n_prob_c),
+        theta_prev = ws_take<double>(n_prob_c),
+        gap = ws_take<double>(n_prob_c);
+    Buf<int> iter = ws_take<int>(1),
+        msteps = ws_take<int>(n_prob_c),
+        conv = ws_take<int>(n_prob_c),
+        active_next = ws_take<int>(nv);
     g_kernels += 1;
     k_bgather_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(
         n_prob_c, NC, nsp_b, lz_base.n_prob, j, d_vs_base.p, d_vs_set.p, d_real.p, lz_base.alpha, lz_base.beta,
@@ -1328,7 +1409,7 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     };
     int done = j;
     {
-        DevBuf<int> d_w(nv);
+        Buf<int> d_w = ws_take<int>(nv);
         d_w.upload(n_real.data(), nv, st);
         LoopOut lo = device_loop(step, ac, lz, NC, stall, res_tol, e_tol, gap_in ? gap.p : nullptr, nullptr, theta.p,
                                  theta_prev.p, msteps.p, conv.p, ck.d_active.p, active_next.p, ck.d_nrows.p, d_w.p,
@@ -1393,10 +1474,18 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     grow(k.ws_w, 2 * (size_t)tot * sizeof(V));
     grow(k.ws_ring, (size_t)K * tot * sizeof(V));
     struct View { V* p; } wbuf{reinterpret_cast<V*>(k.ws_w.p)}, vring{reinterpret_cast<V*>(k.ws_ring.p)};
-    DevBuf<double> alpha((size_t)(cap + 1) * n_prob), beta((size_t)(cap + 2) * n_prob),
-        partials((size_t)std::max(1, k.n_tiles) * b->nsp), theta(n_prob), theta_prev(n_prob),
-        ritz((size_t)(cap + 1) * n_prob), Ls((size_t)(cap + 1) * n_prob), Ds((size_t)(cap + 1) * n_prob);
-    DevBuf<int> iter(1), msteps(n_prob), conv(n_prob), active_next(k.n_sectors);
+    Buf<double> alpha = ws_take<double>((size_t)(cap + 1) * n_prob),
+        beta = ws_take<double>((size_t)(cap + 2) * n_prob),
+        partials = ws_take<double>((size_t)std::max(1, k.n_tiles) * b->nsp),
+        theta = ws_take<double>(n_prob),
+        theta_prev = ws_take<double>(n_prob),
+        ritz = ws_take<double>((size_t)(cap + 1) * n_prob),
+        Ls = ws_take<double>((size_t)(cap + 1) * n_prob),
+        Ds = ws_take<double>((size_t)(cap + 1) * n_prob);
+    Buf<int> iter = ws_take<int>(1),
+        msteps = ws_take<int>(n_prob),
+        conv = ws_take<int>(n_prob),
+        active_next = ws_take<int>(k.n_sectors);
     QMB_CUDA_TRY(cudaMemsetAsync(theta_prev.p, 0, sizeof(double) * n_prob, st));
     QMB_CUDA_TRY(cudaMemsetAsync(conv.p, 0, sizeof(int) * n_prob, st));
     QMB_CUDA_TRY(cudaMemsetAsync(msteps.p, 0, sizeof(int) * n_prob, st));
@@ -1410,15 +1499,17 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
         std::vector<int> ones(k.n_sectors, 1);
         k.d_active.upload(ones.data(), k.n_sectors, st);
     }
-    BatchArgs a = make_args(b, k);
-    a.val = f64 ? k.val64.p : k.val32.p;
-    a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
-    a.dz = f64 ? k.dz64.p : k.dz32.p;
+    // the solver runs on the reverse Cuthill-McKee copy: gathers of nearby
+    // rows hit nearby rows of the vector
+    BatchArgs a = make_args(b, k, true);
+    a.val = f64 ? k.rval64.p : k.rval32.p;
+    a.dxy = f64 ? k.rdxy64.p : k.rdxy32.p;
+    a.dz = f64 ? k.rdz64.p : k.rdz32.p;
     BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob, k.d_sec_ctr.p, k.d_sec_tile0.p, k.d_sec_ntiles.p};
     const int rb = 256, rg = (n_prob + rb - 1) / rb;
     tuned_variant<V>(a, k, f64, st);
     g_kernels += 1;
-    k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
+    k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p, k.d_order.p);
     bnorm0_any<V>(a, k, wbuf.p, lz, st);
     g_kernels += 1;
     k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
@@ -1437,7 +1528,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     }
     {
         std::vector<int> wts(k.n_sectors, b->n_sets);
-        DevBuf<int> d_w(k.n_sectors);
+        Buf<int> d_w = ws_take<int>(k.n_sectors);
         d_w.upload(wts.data(), k.n_sectors, st);
         const bool can_compact = !psi_out && K == 2;
         LoopOut lo = device_loop(step, a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p,
@@ -1487,7 +1578,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     }
     // Ritz vectors (FP64) for the next phase or the caller
     if (psi_out) {
-        DevBuf<double> xs((size_t)(cap + 1) * n_prob);
+        Buf<double> xs = ws_take<double>((size_t)(cap + 1) * n_prob);
         g_kernels += 1;
         k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p, gap_out);
         if (K > 2 && done < K) {
@@ -1499,7 +1590,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             std::vector<int> all(k.n_sectors, 1);
             k.d_active.upload(all.data(), k.n_sectors, st);
             g_kernels += 1;
-            k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
+            k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p, k.d_order.p);
             bnorm0_any<V>(a, k, wbuf.p, lz, st);
             g_kernels += 1;
             k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
@@ -1528,6 +1619,78 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
 
 }  // namespace qmb
 
+// Reverse Cuthill-McKee order of a symmetric sparsity pattern given as CSR
+// (self entries ignored): breadth-first search from a pseudo-peripheral
+// vertex of every connected component, neighbours taken in increasing
+// degree, the whole order reversed.  Returns order[new] = old.  Rows close
+// in this order have close neighbours, so a sweep over the rows gathers
+// from a narrow window of the vector.
+static std::vector<int64_t> rcm_order(const std::vector<int64_t>& rp, const std::vector<uint32_t>& col) {
+    const int64_t n = (int64_t)rp.size() - 1;
+    std::vector<int64_t> deg(n), order;
+    order.reserve(n);
+    for (int64_t i = 0; i < n; ++i) deg[i] = rp[i + 1] - rp[i];
+    std::vector<int64_t> level(n, -1), stamp(n, -1), byd(n);
+    for (int64_t i = 0; i < n; ++i) byd[i] = i;
+    std::stable_sort(byd.begin(), byd.end(), [&](int64_t x, int64_t y) { return deg[x] < deg[y]; });
+    std::vector<char> done(n, 0);
+    std::vector<int64_t> queue, nb;
+    int64_t run = 0;
+    // breadth-first levels of the component of v; returns the min-degree
+    // vertex of the last level and its depth
+    auto bfs_far = [&](int64_t v, int64_t& depth) {
+        ++run;
+        queue.assign(1, v);
+        stamp[v] = run;
+        level[v] = 0;
+        int64_t far = v;
+        for (size_t h = 0; h < queue.size(); ++h) {
+            const int64_t x = queue[h];
+            if (level[x] > level[far] || (level[x] == level[far] && deg[x] < deg[far])) far = x;
+            for (int64_t e = rp[x]; e < rp[x + 1]; ++e) {
+                const int64_t y = col[e];
+                if (y == x || stamp[y] == run) continue;
+                stamp[y] = run;
+                level[y] = level[x] + 1;
+                queue.push_back(y);
+            }
+        }
+        depth = level[far];
+        return far;
+    };
+    for (int64_t k = 0; k < n; ++k) {
+        int64_t v = byd[k];
+        if (done[v]) continue;
+        int64_t depth = 0, d2 = 0;
+        int64_t far = bfs_far(v, depth);
+        for (int it = 0; it < 6; ++it) {
+            const int64_t f2 = bfs_far(far, d2);
+            if (d2 <= depth) break;
+            depth = d2;
+            far = f2;
+        }
+        v = far;
+        const size_t c0 = order.size();
+        order.push_back(v);
+        done[v] = 1;
+        for (size_t h = c0; h < order.size(); ++h) {
+            const int64_t x = order[h];
+            nb.clear();
+            for (int64_t e = rp[x]; e < rp[x + 1]; ++e) {
+                const int64_t y = col[e];
+                if (!done[y]) {
+                    done[y] = 1;
+                    nb.push_back(y);
+                }
+            }
+            std::stable_sort(nb.begin(), nb.end(), [&](int64_t a2, int64_t b2) { return deg[a2] < deg[b2]; });
+            order.insert(order.end(), nb.begin(), nb.end());
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
 // ------------------------------------------------------------------ C ABI
 extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) {
     return guarded([&] {
@@ -1553,6 +1716,11 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             std::vector<uint32_t> col;
             std::vector<double2> val;
             std::vector<double2> dxy, dz;
+            // reverse Cuthill-McKee copy
+            std::vector<int64_t> order, r_row_ptr;
+            std::vector<uint32_t> r_col;
+            std::vector<double2> r_val, r_dxy, r_dz;
+            int64_t bandwidth = 0;
         };
         std::vector<Part> parts(d->n_sectors);
         for (int s = 0; s < d->n_sectors; ++s) {
@@ -1612,6 +1780,31 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             }
             P.dxy = std::move(dx);
             P.dz = std::move(dz);
+            // the same sector in reverse Cuthill-McKee order, columns sorted
+            P.order = rcm_order(P.row_ptr, P.col);
+            std::vector<int64_t> pos(n);
+            for (int64_t i = 0; i < n; ++i) pos[P.order[i]] = i;
+            P.r_row_ptr.assign(1, 0);
+            P.bandwidth = 0;
+            std::vector<std::pair<uint32_t, double2>> rowbuf;
+            for (int64_t i = 0; i < n; ++i) {
+                const int64_t o = P.order[i];
+                rowbuf.clear();
+                for (int64_t e = P.row_ptr[o]; e < P.row_ptr[o + 1]; ++e)
+                    rowbuf.emplace_back((uint32_t)pos[P.col[e]], P.val[e]);
+                std::stable_sort(rowbuf.begin(), rowbuf.end(),
+                                 [](const std::pair<uint32_t, double2>& x, const std::pair<uint32_t, double2>& y) {
+                                     return x.first < y.first;
+                                 });
+                for (auto& pr : rowbuf) {
+                    P.r_col.push_back(pr.first);
+                    P.r_val.push_back(pr.second);
+                    P.bandwidth = std::max<int64_t>(P.bandwidth, std::llabs((int64_t)pr.first - i));
+                }
+                P.r_row_ptr.push_back((int64_t)P.r_col.size());
+                P.r_dxy.push_back(P.dxy[o]);
+                P.r_dz.push_back(P.dz[o]);
+            }
         }
         // assemble the two kinds
         for (int kd = 0; kd < 2; ++kd) {
@@ -1619,6 +1812,9 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             std::vector<int64_t> row_ptr, row_base, row0;
             std::vector<uint32_t> col;
             std::vector<double2> val, dxy, dz;
+            std::vector<int64_t> r_row_ptr, order;
+            std::vector<uint32_t> r_col;
+            std::vector<double2> r_val, r_dxy, r_dz;
             K.sec_elem.assign(1, 0);
             for (int s = 0; s < d->n_sectors; ++s) {
                 if (b->sector_kind[s] != kd) continue;
@@ -1638,6 +1834,13 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                 val.insert(val.end(), P.val.begin(), P.val.end());
                 dxy.insert(dxy.end(), P.dxy.begin(), P.dxy.end());
                 dz.insert(dz.end(), P.dz.begin(), P.dz.end());
+                for (int64_t r = 0; r <= n; ++r) r_row_ptr.push_back(eb + P.r_row_ptr[r]);
+                r_col.insert(r_col.end(), P.r_col.begin(), P.r_col.end());
+                r_val.insert(r_val.end(), P.r_val.begin(), P.r_val.end());
+                r_dxy.insert(r_dxy.end(), P.r_dxy.begin(), P.r_dxy.end());
+                r_dz.insert(r_dz.end(), P.r_dz.begin(), P.r_dz.end());
+                order.insert(order.end(), P.order.begin(), P.order.end());
+                K.bandwidth.push_back(P.bandwidth);
                 K.sec_tile0.push_back((int)K.tile_sector.size());
                 int nt = (int)((n + kBTile - 1) / kBTile);
                 K.sec_ntiles.push_back(nt);
@@ -1647,6 +1850,8 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                     int64_t re = std::min<int64_t>(n, (int64_t)(t + 1) * kBTile);
                     K.max_tile_entries = std::max<int>(K.max_tile_entries,
                                                        (int)(P.row_ptr[re] - P.row_ptr[(int64_t)t * kBTile]));
+                    K.max_tile_entries = std::max<int>(K.max_tile_entries,
+                                                       (int)(P.r_row_ptr[re] - P.r_row_ptr[(int64_t)t * kBTile]));
                 }
             }
             if (!K.n_sectors) continue;
@@ -1698,6 +1903,13 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             store(K.val64, K.val32, val);
             store(K.dxy64, K.dxy32, dxy);
             store(K.dz64, K.dz32, dz);
+            up_l(K.d_rcm_row_ptr, r_row_ptr);
+            up_l(K.d_order, order);
+            K.d_rcm_col.alloc(std::max<size_t>(1, r_col.size()));
+            if (!r_col.empty()) K.d_rcm_col.upload(r_col.data(), r_col.size());
+            store(K.rval64, K.rval32, r_val);
+            store(K.rdxy64, K.rdxy32, r_dxy);
+            store(K.rdz64, K.rdz32, r_dz);
         }
         b->cxy.alloc(b->nsp);
         b->cz.alloc(b->nsp);
@@ -1834,13 +2046,23 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
         const int check = o.check_every > 0 ? o.check_every : 10;
         const double tol64 = o.tol > 0 ? o.tol : 1e-12;
         g_kernels = 0;
+        b->ws.next = 0;
+        g_ws = &b->ws;
+        struct WsGuard {
+            ~WsGuard() { g_ws = nullptr; }
+        } ws_guard;
         int n_hv = 0, it_low = 0, it_tot = 0;
         double products = 0;
         bool all_conv = true;
         std::vector<double> result(b->n_sectors * (size_t)b->n_sets, 0.0), low(result.size(), 0.0);
+        const auto t_solve = std::chrono::steady_clock::now();
+        auto solve_ms = [&]() {
+            return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_solve).count();
+        };
         for (int kd = 0; kd < 2; ++kd) {
             BKind& k = b->kind[kd];
             if (!k.n_sectors) continue;
+            if (trace_on()) std::fprintf(stderr, "[qmb batch] kind %d starts at %.2f ms\n", kd, solve_ms());
             const int64_t tot = k.sec_elem[k.n_sectors];
             const int n_prob = k.n_sectors * b->nsp;
             int64_t minrows = INT64_MAX;
@@ -1853,9 +2075,9 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                 it_low = it_tot;
                 products += ph.products;
             } else {
-                DevBuf<unsigned char> psi(tot * (kd ? 16 : 8));
+                Buf<unsigned char> psi = ws_take<unsigned char>(tot * (kd ? 16 : 8));
                 const int slots = o.mode == QMB_MODE_MIXED ? krylov_slots((size_t)tot * (kd ? 8 : 4), o.max_iter + 1, k.ws_ring.n) : 0;
-                DevBuf<double> gapb((size_t)k.n_sectors * b->nsp);
+                Buf<double> gapb = ws_take<double>((size_t)k.n_sectors * b->nsp);
                 gapb.zero(st);
                 void* psi_out = o.mode == QMB_MODE_MIXED ? (void*)psi.p : nullptr;
                 // FP32 phase: Ritz pair accurate enough that the FP64 restart
@@ -1875,15 +2097,18 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                     const int n_prob = k.n_sectors * b->nsp;
                     std::vector<double> e_rq(n_prob);
                     std::vector<int> act(k.n_sectors, 0);
-                    DevBuf<int> act_d(k.n_sectors), ok(n_prob);
+                    Buf<int> act_d = ws_take<int>(k.n_sectors),
+                        ok = ws_take<int>(n_prob);
                     {
-                        BatchArgs a = make_args(b, k);
-                        a.val = k.val64.p;
-                        a.dxy = k.dxy64.p;
-                        a.dz = k.dz64.p;
-                        DevBuf<unsigned char> hy(tot * (kd ? 16 : 8));
-                        DevBuf<double> part(2 * (size_t)k.n_tiles * b->nsp), sums(2 * (size_t)n_prob),
-                            Eq(n_prob), r2(2 * (size_t)n_prob);
+                        BatchArgs a = make_args(b, k, true);
+                        a.val = k.rval64.p;
+                        a.dxy = k.rdxy64.p;
+                        a.dz = k.rdz64.p;
+                        Buf<unsigned char> hy = ws_take<unsigned char>(tot * (kd ? 16 : 8));
+                        Buf<double> part = ws_take<double>(2 * (size_t)k.n_tiles * b->nsp),
+                            sums = ws_take<double>(2 * (size_t)n_prob),
+                            Eq = ws_take<double>(n_prob),
+                            r2 = ws_take<double>(2 * (size_t)n_prob);
                         BLz lz0{nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr};
                         std::vector<int> ones(k.n_sectors, 1);
                         k.d_active.upload(ones.data(), k.n_sectors, st);
@@ -1942,6 +2167,7 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                         }
                         ++n_hv;
                     }
+                    if (trace_on()) std::fprintf(stderr, "[qmb batch] rq check done at %.2f ms\n", solve_ms());
                     int m2 = o.refine_max_iter > 0 ? o.refine_max_iter : 300;
                     bool any = false;
                     for (int v : act) any |= v != 0;

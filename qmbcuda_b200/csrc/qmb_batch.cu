@@ -421,7 +421,7 @@ __global__ void k_brq_accept(BatchArgs a, int n_prob, int nsets, const double* _
 
 template <class V>
 __global__ void k_bstart(BatchArgs a, int64_t tot, int mode, uint64_t seed, const void* from,
-                         V* __restrict__ w0, const int64_t* __restrict__ order) {
+                         V* __restrict__ w0) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot;
          i += (int64_t)gridDim.x * blockDim.x) {
         V v;
@@ -436,21 +436,8 @@ __global__ void k_bstart(BatchArgs a, int64_t tot, int mode, uint64_t seed, cons
                 z ^= z >> 31;
                 return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
             };
-            // the random value belongs to the (sector, original row, set)
-            // element, whatever the row order of the layout
-            int64_t c = i;
-            if (order) {
-                int lo = 0, hi = a.n_sectors - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (a.sec_elem[mid] <= i) lo = mid;
-                    else hi = mid - 1;
-                }
-                const int64_t loc = i - a.sec_elem[lo];
-                c = a.sec_elem[lo] + order[a.row0[lo] + loc / a.nsp] * a.nsp + loc % a.nsp;
-            }
-            if constexpr (Sc<V>::cplx) v = Sc<V>::from(make_double2(u(2 * c), u(2 * c + 1)));
-            else v = Sc<V>::from(make_double2(u(c), 0.0));
+            if constexpr (Sc<V>::cplx) v = Sc<V>::from(make_double2(u(2 * i), u(2 * i + 1)));
+            else v = Sc<V>::from(make_double2(u(i), 0.0));
         }
         w0[i] = v;
     }
@@ -969,13 +956,6 @@ struct BKind {
     float tune_ms[2][4] = {};
     DevBuf<int64_t> d_sec_elem, d_nrows, d_row_ptr, d_row_base, d_row0;
     std::vector<int64_t> h_row_base, h_row0;  // per sector, as on the device
-    // the same matrices with each sector's rows in reverse Cuthill-McKee order
-    // (same row_base / row0 offsets), used by the solver; order maps an RCM
-    // row to its original row
-    DevBuf<int64_t> d_rcm_row_ptr, d_order;
-    DevBuf<uint32_t> d_rcm_col;
-    DevBuf<unsigned char> rval64, rval32, rdxy64, rdxy32, rdz64, rdz32;
-    std::vector<int64_t> bandwidth;  // per sector, max |col - row| in RCM order
     DevBuf<uint32_t> d_col;
     DevBuf<unsigned char> val64, val32, dxy64, dxy32, dz64, dz32;
     int64_t nnz = 0, rows = 0;
@@ -994,7 +974,7 @@ struct qmb_batch_s {
 
 namespace qmb {
 
-static BatchArgs make_args(const qmb_batch_s* b, const BKind& k, bool rcm = false) {
+static BatchArgs make_args(const qmb_batch_s* b, const BKind& k) {
     BatchArgs a;
     a.n_sectors = k.n_sectors;
     a.nsp = b->nsp;
@@ -1003,10 +983,10 @@ static BatchArgs make_args(const qmb_batch_s* b, const BKind& k, bool rcm = fals
     a.tile_row0 = k.d_tile_row0.p;
     a.sec_elem = k.d_sec_elem.p;
     a.sec_nrows = k.d_nrows.p;
-    a.row_ptr = rcm ? k.d_rcm_row_ptr.p : k.d_row_ptr.p;
+    a.row_ptr = k.d_row_ptr.p;
     a.row_base = k.d_row_base.p;
     a.row0 = k.d_row0.p;
-    a.col = rcm ? k.d_rcm_col.p : k.d_col.p;
+    a.col = k.d_col.p;
     a.val = nullptr;
     a.dxy = nullptr;
     a.dz = nullptr;
@@ -1499,17 +1479,15 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
         std::vector<int> ones(k.n_sectors, 1);
         k.d_active.upload(ones.data(), k.n_sectors, st);
     }
-    // the solver runs on the reverse Cuthill-McKee copy: gathers of nearby
-    // rows hit nearby rows of the vector
-    BatchArgs a = make_args(b, k, true);
-    a.val = f64 ? k.rval64.p : k.rval32.p;
-    a.dxy = f64 ? k.rdxy64.p : k.rdxy32.p;
-    a.dz = f64 ? k.rdz64.p : k.rdz32.p;
+    BatchArgs a = make_args(b, k);
+    a.val = f64 ? k.val64.p : k.val32.p;
+    a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
+    a.dz = f64 ? k.dz64.p : k.dz32.p;
     BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob, k.d_sec_ctr.p, k.d_sec_tile0.p, k.d_sec_ntiles.p};
     const int rb = 256, rg = (n_prob + rb - 1) / rb;
     tuned_variant<V>(a, k, f64, st);
     g_kernels += 1;
-    k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p, k.d_order.p);
+    k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
     bnorm0_any<V>(a, k, wbuf.p, lz, st);
     g_kernels += 1;
     k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
@@ -1590,7 +1568,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             std::vector<int> all(k.n_sectors, 1);
             k.d_active.upload(all.data(), k.n_sectors, st);
             g_kernels += 1;
-            k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p, k.d_order.p);
+            k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, start, seed, psi_in, wbuf.p);
             bnorm0_any<V>(a, k, wbuf.p, lz, st);
             g_kernels += 1;
             k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
@@ -1619,78 +1597,6 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
 
 }  // namespace qmb
 
-// Reverse Cuthill-McKee order of a symmetric sparsity pattern given as CSR
-// (self entries ignored): breadth-first search from a pseudo-peripheral
-// vertex of every connected component, neighbours taken in increasing
-// degree, the whole order reversed.  Returns order[new] = old.  Rows close
-// in this order have close neighbours, so a sweep over the rows gathers
-// from a narrow window of the vector.
-static std::vector<int64_t> rcm_order(const std::vector<int64_t>& rp, const std::vector<uint32_t>& col) {
-    const int64_t n = (int64_t)rp.size() - 1;
-    std::vector<int64_t> deg(n), order;
-    order.reserve(n);
-    for (int64_t i = 0; i < n; ++i) deg[i] = rp[i + 1] - rp[i];
-    std::vector<int64_t> level(n, -1), stamp(n, -1), byd(n);
-    for (int64_t i = 0; i < n; ++i) byd[i] = i;
-    std::stable_sort(byd.begin(), byd.end(), [&](int64_t x, int64_t y) { return deg[x] < deg[y]; });
-    std::vector<char> done(n, 0);
-    std::vector<int64_t> queue, nb;
-    int64_t run = 0;
-    // breadth-first levels of the component of v; returns the min-degree
-    // vertex of the last level and its depth
-    auto bfs_far = [&](int64_t v, int64_t& depth) {
-        ++run;
-        queue.assign(1, v);
-        stamp[v] = run;
-        level[v] = 0;
-        int64_t far = v;
-        for (size_t h = 0; h < queue.size(); ++h) {
-            const int64_t x = queue[h];
-            if (level[x] > level[far] || (level[x] == level[far] && deg[x] < deg[far])) far = x;
-            for (int64_t e = rp[x]; e < rp[x + 1]; ++e) {
-                const int64_t y = col[e];
-                if (y == x || stamp[y] == run) continue;
-                stamp[y] = run;
-                level[y] = level[x] + 1;
-                queue.push_back(y);
-            }
-        }
-        depth = level[far];
-        return far;
-    };
-    for (int64_t k = 0; k < n; ++k) {
-        int64_t v = byd[k];
-        if (done[v]) continue;
-        int64_t depth = 0, d2 = 0;
-        int64_t far = bfs_far(v, depth);
-        for (int it = 0; it < 6; ++it) {
-            const int64_t f2 = bfs_far(far, d2);
-            if (d2 <= depth) break;
-            depth = d2;
-            far = f2;
-        }
-        v = far;
-        const size_t c0 = order.size();
-        order.push_back(v);
-        done[v] = 1;
-        for (size_t h = c0; h < order.size(); ++h) {
-            const int64_t x = order[h];
-            nb.clear();
-            for (int64_t e = rp[x]; e < rp[x + 1]; ++e) {
-                const int64_t y = col[e];
-                if (!done[y]) {
-                    done[y] = 1;
-                    nb.push_back(y);
-                }
-            }
-            std::stable_sort(nb.begin(), nb.end(), [&](int64_t a2, int64_t b2) { return deg[a2] < deg[b2]; });
-            order.insert(order.end(), nb.begin(), nb.end());
-        }
-    }
-    std::reverse(order.begin(), order.end());
-    return order;
-}
-
 // ------------------------------------------------------------------ C ABI
 extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) {
     return guarded([&] {
@@ -1716,11 +1622,6 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             std::vector<uint32_t> col;
             std::vector<double2> val;
             std::vector<double2> dxy, dz;
-            // reverse Cuthill-McKee copy
-            std::vector<int64_t> order, r_row_ptr;
-            std::vector<uint32_t> r_col;
-            std::vector<double2> r_val, r_dxy, r_dz;
-            int64_t bandwidth = 0;
         };
         std::vector<Part> parts(d->n_sectors);
         for (int s = 0; s < d->n_sectors; ++s) {
@@ -1780,31 +1681,6 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             }
             P.dxy = std::move(dx);
             P.dz = std::move(dz);
-            // the same sector in reverse Cuthill-McKee order, columns sorted
-            P.order = rcm_order(P.row_ptr, P.col);
-            std::vector<int64_t> pos(n);
-            for (int64_t i = 0; i < n; ++i) pos[P.order[i]] = i;
-            P.r_row_ptr.assign(1, 0);
-            P.bandwidth = 0;
-            std::vector<std::pair<uint32_t, double2>> rowbuf;
-            for (int64_t i = 0; i < n; ++i) {
-                const int64_t o = P.order[i];
-                rowbuf.clear();
-                for (int64_t e = P.row_ptr[o]; e < P.row_ptr[o + 1]; ++e)
-                    rowbuf.emplace_back((uint32_t)pos[P.col[e]], P.val[e]);
-                std::stable_sort(rowbuf.begin(), rowbuf.end(),
-                                 [](const std::pair<uint32_t, double2>& x, const std::pair<uint32_t, double2>& y) {
-                                     return x.first < y.first;
-                                 });
-                for (auto& pr : rowbuf) {
-                    P.r_col.push_back(pr.first);
-                    P.r_val.push_back(pr.second);
-                    P.bandwidth = std::max<int64_t>(P.bandwidth, std::llabs((int64_t)pr.first - i));
-                }
-                P.r_row_ptr.push_back((int64_t)P.r_col.size());
-                P.r_dxy.push_back(P.dxy[o]);
-                P.r_dz.push_back(P.dz[o]);
-            }
         }
         // assemble the two kinds
         for (int kd = 0; kd < 2; ++kd) {
@@ -1812,9 +1688,6 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             std::vector<int64_t> row_ptr, row_base, row0;
             std::vector<uint32_t> col;
             std::vector<double2> val, dxy, dz;
-            std::vector<int64_t> r_row_ptr, order;
-            std::vector<uint32_t> r_col;
-            std::vector<double2> r_val, r_dxy, r_dz;
             K.sec_elem.assign(1, 0);
             for (int s = 0; s < d->n_sectors; ++s) {
                 if (b->sector_kind[s] != kd) continue;
@@ -1834,13 +1707,6 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                 val.insert(val.end(), P.val.begin(), P.val.end());
                 dxy.insert(dxy.end(), P.dxy.begin(), P.dxy.end());
                 dz.insert(dz.end(), P.dz.begin(), P.dz.end());
-                for (int64_t r = 0; r <= n; ++r) r_row_ptr.push_back(eb + P.r_row_ptr[r]);
-                r_col.insert(r_col.end(), P.r_col.begin(), P.r_col.end());
-                r_val.insert(r_val.end(), P.r_val.begin(), P.r_val.end());
-                r_dxy.insert(r_dxy.end(), P.r_dxy.begin(), P.r_dxy.end());
-                r_dz.insert(r_dz.end(), P.r_dz.begin(), P.r_dz.end());
-                order.insert(order.end(), P.order.begin(), P.order.end());
-                K.bandwidth.push_back(P.bandwidth);
                 K.sec_tile0.push_back((int)K.tile_sector.size());
                 int nt = (int)((n + kBTile - 1) / kBTile);
                 K.sec_ntiles.push_back(nt);
@@ -1850,8 +1716,6 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                     int64_t re = std::min<int64_t>(n, (int64_t)(t + 1) * kBTile);
                     K.max_tile_entries = std::max<int>(K.max_tile_entries,
                                                        (int)(P.row_ptr[re] - P.row_ptr[(int64_t)t * kBTile]));
-                    K.max_tile_entries = std::max<int>(K.max_tile_entries,
-                                                       (int)(P.r_row_ptr[re] - P.r_row_ptr[(int64_t)t * kBTile]));
                 }
             }
             if (!K.n_sectors) continue;
@@ -1903,13 +1767,6 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             store(K.val64, K.val32, val);
             store(K.dxy64, K.dxy32, dxy);
             store(K.dz64, K.dz32, dz);
-            up_l(K.d_rcm_row_ptr, r_row_ptr);
-            up_l(K.d_order, order);
-            K.d_rcm_col.alloc(std::max<size_t>(1, r_col.size()));
-            if (!r_col.empty()) K.d_rcm_col.upload(r_col.data(), r_col.size());
-            store(K.rval64, K.rval32, r_val);
-            store(K.rdxy64, K.rdxy32, r_dxy);
-            store(K.rdz64, K.rdz32, r_dz);
         }
         b->cxy.alloc(b->nsp);
         b->cz.alloc(b->nsp);
@@ -2100,10 +1957,10 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                     Buf<int> act_d = ws_take<int>(k.n_sectors),
                         ok = ws_take<int>(n_prob);
                     {
-                        BatchArgs a = make_args(b, k, true);
-                        a.val = k.rval64.p;
-                        a.dxy = k.rdxy64.p;
-                        a.dz = k.rdz64.p;
+                        BatchArgs a = make_args(b, k);
+                        a.val = k.val64.p;
+                        a.dxy = k.dxy64.p;
+                        a.dz = k.dz64.p;
                         Buf<unsigned char> hy = ws_take<unsigned char>(tot * (kd ? 16 : 8));
                         Buf<double> part = ws_take<double>(2 * (size_t)k.n_tiles * b->nsp),
                             sums = ws_take<double>(2 * (size_t)n_prob),

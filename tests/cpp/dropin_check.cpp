@@ -1,0 +1,129 @@
+// Uses include/qmb/qmbcuda.hpp the way the reference's examples use its
+// classes and checks the energies.  Exit code 0 when every check passes.
+//
+//  1. L=12 chain from T_standard (both bond directions, reference weights),
+//     all 12 translation irreps: lowest energy -4.7747818349 (= 2 E + L/2 of
+//     the physical Heisenberg chain, E = -5.3873909174).
+//  2. The same chain without symmetry (HeisenbergHam_CUDA) gives the same.
+//  3. 4x3 open square lattice with J2: the union of the C2 irreps
+//     (Cn_group about the central point) equals the unsymmetrised result.
+//  4. Heisenberg model with +-x Jxy rows of J/2 and Jz = J: physical chain
+//     energy -5.3873909174 from HeisenbergXXZAbelianSymms_CUDA.
+//  5. LanczosEigVals_CUDA on a reference-layout ELL (k=0 irrep) agrees with
+//     the k=0 energy of check 4 within FP32, 120 fixed steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "qmb/qmbcuda.hpp"
+
+static int fails = 0;
+
+static void expect(const char* name, double got, double want, double tol) {
+    const bool ok = std::fabs(got - want) <= tol * std::max(1.0, std::fabs(want));
+    std::printf("%s %.10f want %.10f %s\n", name, got, want, ok ? "ok" : "FAIL");
+    if (!ok) ++fails;
+}
+
+static float lowest(const std::vector<std::vector<float>>& E) {
+    float m = 1e30f;
+    for (const auto& row : E) m = std::min(m, row[0]);
+    return m;
+}
+
+static int run();
+
+int main() {
+    std::setvbuf(stdout, nullptr, _IONBF, 0);
+    try {
+        return run();
+    } catch (const std::exception& e) {
+        std::printf("exception: %s\nFAILED\n", e.what());
+        return 1;
+    }
+}
+
+static int run() {
+    const int L = 12;
+    LatticeGeometryInfo chain = create_square_lattice_info(L, 1);
+    std::vector<float> B(L, 0.0f), Jw = {1.0f, 1.0f, 1.0f};
+
+    // 1. T_standard + translations
+    T_standard<qmb_complex> TLat(chain, {qmb_complex(1.0f, 0.0f)}, {1.0001f}, 1, 1);
+    Tnm_group T(chain);
+    HeisenbergHamAbelianSymms_CUDA<qmb_complex> Ham(TLat, B, Jw, L / 2, &T, 9);
+    expect("tstandard_translations", lowest(Ham.get_E_vecs()), -4.7747818349, 2e-6);
+
+    // 2. no symmetry
+    T_standard<float> TLatF(chain, {1.0f}, {1.0001f}, 1, 1);
+    HeisenbergHam_CUDA brute(TLatF, B, Jw, L / 2, 9);
+    expect("tstandard_no_symmetry", brute.get_E(), -4.7747818349, 2e-6);
+
+    // 3. C2 on an open 4x3 square lattice with J2
+    LatticeGeometryInfo sq = create_square_lattice_info(4, 3);
+    T_standard<qmb_complex> TS(sq, {qmb_complex(1.0f, 0.0f), qmb_complex(0.15f, 0.0f)}, {1.0001f, 1.4143f}, 1, 0);
+    T_standard<float> TSF(sq, {1.0f, 0.15f}, {1.0001f, 1.4143f}, 1, 0);
+    Cn_group C2(2, TS.GetCentralPoint());
+    HeisenbergHamAbelianSymms_CUDA<qmb_complex> HamC2(TS, std::vector<float>(12, 0.0f), Jw, 6, &C2, 9);
+    HeisenbergHam_CUDA bruteSq(TSF, std::vector<float>(12, 0.0f), Jw, 6, 9);
+    expect("c2_union_equals_full_sector", lowest(HamC2.get_E_vecs()), bruteSq.get_E(), 2e-6);
+
+    // 4. Heisenberg model in the physical convention
+    HeisenbergInfo<qmb_complex> hi;
+    hi.Jxy_terms = {{1, 0, 0, 0}, {-1, 0, 0, 0}};
+    hi.Jxy_couplings = {qmb_complex(0.5f, 0.0f), qmb_complex(0.5f, 0.0f)};
+    hi.Jz_terms = {{1, 0, 0, 0}};
+    hi.Jz_couplings = {1.0f};
+    hi.intra_c_bool = true;
+    hi.inter_c_bool = true;
+    Heisenberg<qmb_complex> model(chain, hi);
+    HeisenbergXXZAbelianSymms_CUDA<qmb_complex> xxz(model, &T);
+    const std::vector<std::vector<float>> Ex = xxz.get_E_vecs();
+    expect("heisenberg_model", lowest(Ex), -5.3873909174, 2e-6);
+
+    // 5. LanczosEigVals_CUDA on the k = 0 reference-layout ELL
+    std::vector<uint32_t> perm((size_t)L * L);
+    T.GetGroupElemArr(model.GetR1(), model.GetR2(), perm.data());
+    qmb_sector_desc d = {L, L / 2, L, perm.data(), 0, 0};
+    qmb_sector s = nullptr;
+    qmb_dropin::check(qmb_sector_create(&d, &s));
+    std::vector<double> ch(2 * L, 0.0);
+    for (int g = 0; g < L; ++g) ch[2 * g] = 1.0;
+    qmb_dropin::check(qmb_sector_set_irrep(s, ch.data(), 1e-5));
+    qmb_sector_info si;
+    qmb_dropin::check(qmb_sector_get_info(s, &si));
+    const int R = (int)si.n_orbits, W = 2 * L + 1;
+    const qmb_terms tt = model.terms();
+    std::vector<uint32_t> ind((size_t)R * W);
+    std::vector<double> val(2 * (size_t)R * W);
+    std::vector<int16_t> track(R);
+    qmb_dropin::check(qmb_ham_export_ref(s, &tt, W, ind.data(), val.data(), track.data()));
+    qmb_sector_destroy(s);
+    std::vector<float> valf((size_t)R * W);
+    for (size_t i = 0; i < valf.size(); ++i) valf[i] = (float)val[2 * i];
+    uint32_t* dind = nullptr;
+    float* dval = nullptr;
+    short* dtr = nullptr;
+    if (cudaMalloc(&dind, ind.size() * 4) != cudaSuccess || cudaMalloc(&dval, valf.size() * 4) != cudaSuccess ||
+        cudaMalloc(&dtr, track.size() * 2) != cudaSuccess) {
+        std::printf("cudaMalloc failed\n");
+        return 2;
+    }
+    cudaMemcpy(dind, ind.data(), ind.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dval, valf.data(), valf.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dtr, track.data(), track.size() * 2, cudaMemcpyHostToDevice);
+    float E = 0.0f;
+    std::vector<float> kry(120);
+    const float res = LanczosEigVals_CUDA<float>(&E, 1, 120, R, W, 2212456, dind, dval, dtr, kry.data(), true, true);
+    cudaFree(dind);
+    cudaFree(dval);
+    cudaFree(dtr);
+    expect("lanczos_eigvals_k0", E, Ex[0][0], 1e-5);
+    std::printf("lanczos_eigvals_residual %.3e %s\n", res, res < 1e-4f ? "ok" : "FAIL");
+    if (!(res < 1e-4f)) ++fails;
+    std::printf("%s\n", fails ? "FAILED" : "PASSED");
+    return fails ? 1 : 0;
+}

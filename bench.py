@@ -1,21 +1,19 @@
 """Benchmark of the XXZ Lanczos ground-state path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Metric (the reference project's headline): H*v/s and HBM GB/s, mixed vs FP64
 at |dE0| < 1e-9; batched sectors/s.  A "step" is one complete ground-state
-solve of the workload.  Workloads (synthetic, seeded):
+solve of the workload (synthetic, seeded):
 
-  batched (default)  256 XXZ chains L=20, periodic, Delta ~ U(0,2), J ~ U(0.5,1.5)
-                     (mt19937-64 seed 20261203), every momentum sector k=0..19 of Sz=0,
-                     one batched mixed-precision Lanczos (FP32 vectors/values, FP64
-                     scalars, FP64 refinement restart)
-  l24                L=24 XXZ chain, J=1, Delta=0.5, k=0, spin-inversion even (56,450 rows),
-                     mixed precision
-  l16                L=16 Heisenberg chain, full Sz=0 sector, FP64, 150 steps, full
-                     reorthogonalisation
-  l32                L=32 J1-J2 chain (1, 0.5), Delta=1, k=0, even, FP32 vectors with FP64
-                     reductions + refinement, 300 steps max, matrix-free H*v optional
+  batched            256 XXZ chains L=20, periodic, Delta ~ U(0,2), J ~ U(0.5,1.5)
+                     (mt19937-64 seed 20261203 + rank), every momentum sector k=0..19
+                     of Sz=0, one batched mixed-precision Lanczos (FP32 vectors/values,
+                     FP64 scalars, FP64 refinement restart)
+
+The single-sector workloads (L=16 without symmetry, L=24 k=0 even, L=32
+J1-J2, 6x6) are parity tests at full size (tests/test_gpu_lanczos.py,
+tests/test_gpu_configs.py).
 
 `value` counts sector H*v products (one coupling set x one sector x one
 product) per second of device time with inputs resident; `e2e` is the same

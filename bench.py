@@ -145,6 +145,43 @@ def time_batch_hv(torch, q, b, prec, reps=20):
     return e0.elapsed_time(e1) / reps
 
 
+def single_sector_hv(torch, q, reps=10):
+    """Stored FP32 H*v of one large sector (L=32 J1-J2 chain, J2 = 0.5,
+    Delta = 1, k = 0, spin-inversion even; 9,393,119 rows): CUDA-event time
+    per product and its algorithmic bytes (qmb_ham_info.bytes_fp32)."""
+    A = q._capi
+    L = 32
+    perm, ch = q.translation_group(L)
+    s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+    J = [1.0] * L + [0.5] * L
+    h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J), prec=A.PREC_FP32)
+    info = h.info
+    x = torch.randn(int(info.n_rows), dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    st = torch.cuda.current_stream()
+    args = (h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), A.C.c_void_p(st.cuda_stream))
+    for _ in range(3):
+        q.check(q.lib().qmb_hv(*args))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(reps):
+        q.check(q.lib().qmb_hv(*args))
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    peak, kind = load_peaks()
+    gbs = info.bytes_fp32 / (ms * 1e-3) / 1e9
+    out = {"workload": "L=32 J1-J2 chain, k=0, even (9,393,119 rows), stored FP32 sliced ELL",
+           "kernel": "k_hv<SellOp<float>>", "rows": int(info.n_rows), "nnz": int(info.nnz_offdiag),
+           "bytes": float(info.bytes_fp32), "ms": ms, "achieved_gbs": gbs, "frac": gbs / peak,
+           "peak_source": kind}
+    h.close()
+    s.close()
+    return out
+
+
 def run_batched(args, torch, q, rank, world):
     A = q._capi
     L, n_sets = 20, 256
@@ -201,6 +238,7 @@ def run_batched(args, torch, q, rank, world):
         for s in s2:
             s.close()
     e2e_s = float(np.mean(e2e_t)) if e2e_t else float("nan")
+    single = None if args.no_compare else single_sector_hv(torch, q)
     out = {
         "workload": "batched: 256 XXZ chains L=20 periodic, Delta~U(0,2), J~U(0.5,1.5) "
                     "(mt19937-64 seed 20261203), all k=0..19 of Sz=0, mixed precision",
@@ -224,6 +262,8 @@ def run_batched(args, torch, q, rank, world):
                      "ms_fp32": [round(v, 4) for v in b.info.tune_ms_fp32],
                      "ms_fp64": [round(v, 4) for v in b.info.tune_ms_fp64],
                      "variants": "(unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4)"},
+        "single_sector_hv": single,
+        "ms_steps": [round(float(v), 2) for v in dev_ms],
         "iters_mixed": [int(r.iters_low), int(r.iters)], "iters_fp64": int(r64.iters),
         "E0_min": float(E_mix.min()),
     }

@@ -17,6 +17,13 @@
  *   HeisenbergXXZAbelianSymms_CUDA<T>                  exact_diagonalization/HeisenbergGenericXXZ_AbelianSymms_CUDA.h:26-89
  *   HeisenbergHam_CUDA                                 exact_diagonalization/HeisenbergHam_CUDA.h:9-31
  *   LanczosEigVals_CUDA<T>                             exact_diagonalization/lanczos.h:20-32
+ *   LanczosEigenStateFromSeed<T>                       exact_diagonalization/lanczos.cu:31-104
+ *   ComputeStaticExpValZeroT (both symmetric drivers)  HeisenbergGenericXXZ_AbelianSymms_CUDA.h:47,
+ *                                                      HeisenbergHamAbelianSymms_CUDA.h:32
+ *   OperatorType, Operator<T>                          quantum_operators/SingleParticleOperators.h
+ *   ManyBodyOperator<T>, Sz, Sp, Sm, SzSz_correlator,
+ *   FourierOperator, FullFourierOperator               quantum_operators/ArbitraryOperator.h
+ *   ReciprocalBasisVectors, SimpleFourierTransform     geometry/base.h:13,15
  *
  * Differences a caller sees:
  *  - No Armadillo.  A group element is a coordinate map (SiteMap: site
@@ -32,12 +39,20 @@
  *  - Errors throw std::runtime_error with the library's message (the
  *    reference throws from its CHECK macros or exits).
  *  - NStates > 1 (excited states) is not supported and throws.
+ *  - ComputeStaticExpValZeroT works on the ground state the constructor kept
+ *    (no rebuild, no second Lanczos pass) and returns the exact expectation
+ *    value also for S+/S- factors, where the reference's kernel drops terms.
+ *    Fermion and boson operator types are rejected (the reference applies
+ *    them as Sz); OperatorType::I is the identity.
+ *  - SimpleFourierTransform takes and returns nested vectors [N1][N2].
  */
 #ifndef QMB_QMBCUDA_HPP
 #define QMB_QMBCUDA_HPP
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
+#include <memory>
 #include <cstdint>
 #include <cstdio>
 #include <functional>
@@ -402,15 +417,333 @@ protected:
     std::vector<float> R0;
 };
 
+// ----------------------------------------------------------------- operators
+// Single-site operator types; the values are the QMB_OP_* codes of qmb_terms.
+enum class OperatorType { Sz, Sp, Sm, c_up, c_dag_up, c_down, c_dag_down, b, b_dag, I };
+
+// One factor: type, lattice site and a scalar (quantum_operators/SingleParticleOperators.h).
+template <typename T>
+class Operator {
+public:
+    Operator(int site_in, OperatorType type_in, T scalar_in) : site(site_in), scalar(scalar_in), type(type_in) {}
+    virtual ~Operator() {}
+    int GetSite() const { return site; }
+    T GetScalar() const { return scalar; }
+    OperatorType GetType() const { return type; }
+    void SetScalar(T s) { scalar = s; }
+    void SetSite(int s) { site = s; }
+
+protected:
+    int site;
+    T scalar;
+    OperatorType type;
+};
+
+// A sum of products of single-site operators (quantum_operators/ArbitraryOperator.h):
+// elements[t] is the product elements[t][0] * elements[t][1] * ...
+template <typename T>
+class ManyBodyOperator {
+public:
+    ManyBodyOperator() {}
+    ManyBodyOperator(std::vector<std::vector<Operator<T>>> elements_in) : elements(std::move(elements_in)) {}
+    virtual ~ManyBodyOperator() {}
+    std::vector<std::vector<Operator<T>>> GetElems() const { return elements; }
+    int GetMaxTerms() const {
+        size_t m = 0;
+        for (const auto& t : elements) m = std::max(m, t.size());
+        return (int)m;
+    }
+    void AddTerm(std::vector<Operator<T>> term) { elements.push_back(std::move(term)); }
+    void AddSingleOperator(Operator<T> op) { elements.push_back({op}); }
+    // Every factor of every term moved to new_site (ArbitraryOperator.cu:58-65).
+    void LocalizeOperator(int new_site) {
+        for (auto& t : elements)
+            for (auto& op : t) op.SetSite(new_site);
+    }
+    ManyBodyOperator<T> operator+(const ManyBodyOperator<T>& A) const {
+        std::vector<std::vector<Operator<T>>> e = elements;
+        for (const auto& t : A.elements) e.push_back(t);
+        return ManyBodyOperator<T>(e);
+    }
+    // Products of all term pairs, factors of this operator first.
+    ManyBodyOperator<T> operator*(const ManyBodyOperator<T>& A) const {
+        std::vector<std::vector<Operator<T>>> e;
+        for (const auto& a : elements)
+            for (const auto& b : A.elements) {
+                std::vector<Operator<T>> t = a;
+                t.insert(t.end(), b.begin(), b.end());
+                e.push_back(t);
+            }
+        return ManyBodyOperator<T>(e);
+    }
+    // A scalar multiplies the first factor of every term.
+    ManyBodyOperator<T> operator*(float s) const {
+        std::vector<std::vector<Operator<T>>> e = elements;
+        for (auto& t : e)
+            if (!t.empty()) t[0].SetScalar(t[0].GetScalar() * T(s));
+        return ManyBodyOperator<T>(e);
+    }
+    ManyBodyOperator<qmb_complex> operator*(qmb_complex s) const {
+        std::vector<std::vector<Operator<qmb_complex>>> e;
+        for (const auto& t : elements) {
+            std::vector<Operator<qmb_complex>> u;
+            for (size_t j = 0; j < t.size(); ++j) {
+                qmb_complex c = qmb_dropin::make_scalar<qmb_complex>::from(qmb_dropin::re(t[j].GetScalar()),
+                                                                           qmb_dropin::im(t[j].GetScalar()));
+                if (j == 0) c = c * s;
+                u.emplace_back(t[j].GetSite(), t[j].GetType(), c);
+            }
+            e.push_back(u);
+        }
+        return ManyBodyOperator<qmb_complex>(e);
+    }
+    void PrintOperator() const {
+        static const char* nm[] = {"Sz", "Sp", "Sm", "c_up", "c_dag_up", "c_down", "c_dag_down", "b", "b_dag", "I"};
+        for (size_t i = 0; i < elements.size(); ++i) {
+            double sr = 1.0, si = 0.0;
+            for (const auto& op : elements[i]) {
+                const double a = qmb_dropin::re(op.GetScalar()), b = qmb_dropin::im(op.GetScalar());
+                const double r = sr * a - si * b;
+                si = sr * b + si * a;
+                sr = r;
+            }
+            if (sr != 1.0 || si != 0.0) std::printf("(%g%+gi) ", sr, si);
+            for (const auto& op : elements[i]) std::printf("%s(r=%d)", nm[(int)op.GetType()], op.GetSite());
+            if (i + 1 < elements.size()) std::printf(" + ");
+        }
+        std::printf("\n");
+    }
+
+protected:
+    std::vector<std::vector<Operator<T>>> elements;
+};
+
+template <typename T>
+ManyBodyOperator<T> operator*(float s, const ManyBodyOperator<T>& A) {
+    return A * s;
+}
+template <typename T>
+ManyBodyOperator<qmb_complex> operator*(qmb_complex s, const ManyBodyOperator<T>& A) {
+    return A * s;
+}
+
+template <typename T>
+class Sz : public ManyBodyOperator<T> {
+public:
+    Sz(int i) { this->elements.push_back({Operator<T>(i, OperatorType::Sz, T(1.0f))}); }
+};
+template <typename T>
+class Sp : public ManyBodyOperator<T> {
+public:
+    Sp(int i) { this->elements.push_back({Operator<T>(i, OperatorType::Sp, T(1.0f))}); }
+};
+template <typename T>
+class Sm : public ManyBodyOperator<T> {
+public:
+    Sm(int i) { this->elements.push_back({Operator<T>(i, OperatorType::Sm, T(1.0f))}); }
+};
+template <typename T>
+class SzSz_correlator : public ManyBodyOperator<T> {
+public:
+    SzSz_correlator(int i, int j) {
+        this->elements.push_back({Operator<T>(i, OperatorType::Sz, T(1.0f)), Operator<T>(j, OperatorType::Sz, T(1.0f))});
+    }
+};
+
+typedef ManyBodyOperator<qmb_complex> ManyBodyOperatorC;
+
+// The reference's B_mat (geometry/base.cpp:7-16): its columns b1, b2 satisfy
+// a_i . b_j = 2 pi delta_ij for the columns a1, a2 of A_mat.
+inline std::vector<std::vector<float>> ReciprocalBasisVectors(LatticeGeometryInfo geom_info) {
+    const auto& A = geom_info.A_mat;
+    const float det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    const float c = 2.0f * 3.14159265358979323846f / det;
+    return {{c * A[1][1], -c * A[1][0]}, {-c * A[0][1], c * A[0][0]}};
+}
+
+// A_k[alpha] = N^-1/2 sum_cells e^{i k.r} A(site), r = i a1 + j a2, site =
+// alpha + (i N2 + j) n_sub, with A localized to the site (ArbitraryOperator.cu:246-282).
+inline std::vector<ManyBodyOperatorC> FourierOperator(ManyBodyOperatorC A, std::vector<float> k,
+                                                      LatticeGeometryInfo geom_info) {
+    const auto& M = geom_info.A_mat;
+    const int N1 = geom_info.N1, N2 = geom_info.N2, ns = (int)geom_info.rx_alpha.size();
+    std::vector<ManyBodyOperatorC> out(ns);
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N2; ++j) {
+            const float rx = i * M[0][0] + j * M[0][1], ry = i * M[1][0] + j * M[1][1];
+            const float ph = k[0] * rx + k[1] * ry;
+            const qmb_complex e = qmb_dropin::make_scalar<qmb_complex>::from(std::cos(ph), std::sin(ph));
+            for (int a = 0; a < ns; ++a) {
+                ManyBodyOperatorC loc = A;
+                loc.LocalizeOperator(a + (i * N2 + j) * ns);
+                out[a] = out[a] + loc * e;
+            }
+        }
+    const qmb_complex nrm = qmb_dropin::make_scalar<qmb_complex>::from(1.0 / std::sqrt((double)(N1 * N2)), 0.0);
+    for (auto& o : out) o = o * nrm;
+    return out;
+}
+
+// FourierOperator at every k = i b1 / N1 + j b2 / N2 ([N1][N2][n_sub]);
+// neg_sqn gives -k (ArbitraryOperator.cu:284-308).
+inline std::vector<std::vector<std::vector<ManyBodyOperatorC>>> FullFourierOperator(ManyBodyOperatorC A,
+                                                                                   LatticeGeometryInfo geom_info,
+                                                                                   bool neg_sqn = false) {
+    const auto B = ReciprocalBasisVectors(geom_info);
+    const int N1 = geom_info.N1, N2 = geom_info.N2;
+    std::vector<std::vector<std::vector<ManyBodyOperatorC>>> out(N1);
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N2; ++j) {
+            std::vector<float> k = {i * B[0][0] / (float)N1 + j * B[0][1] / (float)N2,
+                                    i * B[1][0] / (float)N1 + j * B[1][1] / (float)N2};
+            if (neg_sqn) k = {-k[0], -k[1]};
+            out[i].push_back(FourierOperator(A, k, geom_info));
+        }
+    return out;
+}
+
+// Discrete Fourier transform of an [N1][N2] real-space table to [N1][N2] in k
+// (geometry/base.cpp:18-50), on nested vectors instead of an Armadillo matrix.
+inline std::vector<std::vector<std::complex<float>>> SimpleFourierTransform(
+    const std::vector<std::vector<std::complex<float>>>& A_real_space, LatticeGeometryInfo geom_info) {
+    const auto B = ReciprocalBasisVectors(geom_info);
+    const auto& M = geom_info.A_mat;
+    const int N1 = geom_info.N1, N2 = geom_info.N2;
+    const float div = 1.0f / std::sqrt((float)(N1 * N2));
+    std::vector<std::vector<std::complex<float>>> out(N1, std::vector<std::complex<float>>(N2));
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N2; ++j) {
+            const float rx = i * M[0][0] + j * M[0][1], ry = i * M[1][0] + j * M[1][1];
+            for (int ki = 0; ki < N1; ++ki)
+                for (int kj = 0; kj < N2; ++kj) {
+                    const float kx = ki * B[0][0] / (float)N1 + kj * B[0][1] / (float)N2;
+                    const float ky = ki * B[1][0] / (float)N1 + kj * B[1][1] / (float)N2;
+                    const float ph = kx * rx + ky * ry;
+                    out[ki][kj] += div * std::complex<float>(std::cos(ph), std::sin(ph)) * A_real_space[i][j];
+                }
+        }
+    return out;
+}
+
 // -------------------------------------------------------------------- drivers
 namespace qmb_dropin {
 
+// Owned copy of operator tables.
+struct TermsCopy {
+    std::vector<int> n_ops, op_code, op_site;
+    std::vector<double> scalar;
+    int n_terms = 0, n_col = 1;
+    TermsCopy() {}
+    explicit TermsCopy(const qmb_terms& t) : n_terms(t.n_terms), n_col(t.n_col) {
+        n_ops.assign(t.n_ops, t.n_ops + t.n_terms);
+        op_code.assign(t.op_code, t.op_code + (size_t)t.n_terms * t.n_col);
+        op_site.assign(t.op_site, t.op_site + (size_t)t.n_terms * t.n_col);
+        scalar.assign(t.scalar, t.scalar + 2 * (size_t)t.n_terms);
+    }
+    qmb_terms view() const {
+        qmb_terms t;
+        t.n_terms = n_terms;
+        t.n_col = n_col;
+        t.n_ops = n_ops.data();
+        t.op_code = op_code.data();
+        t.op_site = op_site.data();
+        t.scalar = scalar.data();
+        return t;
+    }
+};
+
+// The ground state over all irreps, kept for ComputeStaticExpValZeroT: the
+// sector and irrep it lives in, the Hamiltonian tables and the FP64 vector.
+// The sector and matrix handles are rebuilt on first use and then reused.
+struct GroundState {
+    int irrep = -1;
+    float E = 1.0e7f;
+    int L = 0, n_up = 0, n_perm = 0;
+    float tol_norm = 1e-5f;
+    std::vector<uint32_t> perm;
+    std::vector<double> chars;  // complex row of the irrep
+    TermsCopy terms;
+    std::vector<double> psi;    // FP64, complex interleaved when the matrix is complex
+    int64_t n_rows = 0;
+    struct Handles {
+        qmb_sector s = nullptr;
+        qmb_ham h = nullptr;
+        ~Handles() {
+            if (h) qmb_ham_destroy(h);
+            if (s) qmb_sector_destroy(s);
+        }
+    };
+    std::shared_ptr<Handles> hd;
+
+    qmb_ham ham() {
+        if (irrep < 0) throw std::runtime_error("qmb: no ground state was found");
+        if (hd) return hd->h;
+        auto H = std::make_shared<Handles>();
+        qmb_sector_desc d;
+        d.L = L;
+        d.n_up = n_up;
+        d.n_perm = n_perm;
+        d.perm = perm.data();
+        d.spin_flip = 0;
+        d.device = 0;
+        check(qmb_sector_create(&d, &H->s));
+        check(qmb_sector_set_irrep(H->s, chars.data(), tol_norm));
+        const qmb_terms t = terms.view();
+        check(qmb_ham_create(H->s, &t, QMB_PREC_FP64, &H->h));
+        check(qmb_set_ground_state(H->h, psi.data(), n_rows));
+        hd = H;
+        return hd->h;
+    }
+};
+
+// <GS|A|GS> through qmb_expval: the tables ComputeStaticExpValZeroT builds
+// (HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:434-455), factors daggered and
+// the scalar conjugated.
+template <class T>
+inline qmb_complex expval(GroundState& gs, const ManyBodyOperator<T>& A) {
+    const auto el = A.GetElems();
+    const int n_col = std::max(1, A.GetMaxTerms());
+    if (n_col > 8) throw std::runtime_error("qmb: a term has more than 8 factors");
+    std::vector<int> n_ops(el.size()), code(el.size() * n_col, 0), site(el.size() * n_col, 0);
+    std::vector<double> sc(2 * el.size());
+    for (size_t i = 0; i < el.size(); ++i) {
+        n_ops[i] = (int)el[i].size();
+        double r = 1.0, m = 0.0;
+        for (size_t j = 0; j < el[i].size(); ++j) {
+            const OperatorType ty = el[i][j].GetType();
+            int c = (int)ty;
+            if (ty == OperatorType::Sp) c = QMB_OP_SM;
+            else if (ty == OperatorType::Sm) c = QMB_OP_SP;
+            code[i * n_col + j] = c;
+            site[i * n_col + j] = el[i][j].GetSite();
+            const double a = re(el[i][j].GetScalar()), b = -im(el[i][j].GetScalar());
+            const double nr = r * a - m * b;
+            m = r * b + m * a;
+            r = nr;
+        }
+        sc[2 * i] = r;
+        sc[2 * i + 1] = m;
+    }
+    qmb_terms t;
+    t.n_terms = (int)el.size();
+    t.n_col = n_col;
+    t.n_ops = n_ops.data();
+    t.op_code = code.data();
+    t.op_site = site.data();
+    t.scalar = sc.data();
+    double out[2] = {0.0, 0.0};
+    check(qmb_expval(gs.ham(), 1, &t, nullptr, out));
+    return make_scalar<qmb_complex>::from(out[0], out[1]);
+}
+
 // Lowest energy of every irrep of G for the given operator tables (one
-// sector handle, one Hamiltonian per irrep, mixed-precision Lanczos).
+// sector handle, one Hamiltonian per irrep, mixed-precision Lanczos).  With
+// gs, the lowest state over all irreps is kept there.
 template <class T>
 inline std::vector<std::vector<float>> solve_irreps(int L, int n_up, SymmetryClass<T>* G, const std::vector<float>& R1,
                                                     const std::vector<float>& R2, const qmb_terms& terms,
-                                                    long long seed, float tol_norm, int NStates) {
+                                                    long long seed, float tol_norm, int NStates,
+                                                    GroundState* gs = nullptr) {
     if (NStates != 1) throw std::runtime_error("qmb: only NStates = 1 (ground states) is supported");
     const int nG = G->GetGroupSize();
     std::vector<uint32_t> perm((size_t)nG * L);
@@ -443,8 +776,21 @@ inline std::vector<std::vector<float>> solve_irreps(int L, int n_up, SymmetryCla
             qmb_lanczos_default_opts(&o);
             o.mode = QMB_MODE_MIXED;
             o.seed = (uint64_t)seed;
+            o.want_vector = gs ? 1 : 0;
             qmb_lanczos_result r;
-            const qmb_status st = qmb_lanczos(h, &o, &r, nullptr, 0);
+            qmb_status st = qmb_lanczos(h, &o, &r, nullptr, 0);
+            if (st == QMB_OK && gs && (float)r.E0 < gs->E) {
+                qmb_ham_info hi;
+                st = qmb_ham_get_info(h, &hi);
+                if (st == QMB_OK) {
+                    gs->psi.assign((hi.is_complex ? 2 : 1) * (size_t)hi.n_rows, 0.0);
+                    st = qmb_ground_state(h, gs->psi.data(), hi.n_rows);
+                    gs->n_rows = hi.n_rows;
+                    gs->E = (float)r.E0;
+                    gs->irrep = (int)a;
+                    gs->chars = c;
+                }
+            }
             qmb_ham_destroy(h);
             check(st);
             E[a][0] = (float)r.E0;
@@ -454,6 +800,15 @@ inline std::vector<std::vector<float>> solve_irreps(int L, int n_up, SymmetryCla
         throw;
     }
     qmb_sector_destroy(s);
+    if (gs) {
+        gs->L = L;
+        gs->n_up = n_up;
+        gs->n_perm = nG;
+        gs->perm = perm;
+        gs->tol_norm = tol_norm;
+        gs->terms = TermsCopy(terms);
+        gs->hd.reset();
+    }
     return E;
 }
 
@@ -509,16 +864,24 @@ public:
         if (J_dim_weights.size() < 3) throw std::runtime_error("qmb: J_dim_weights needs {Jx, Jy, Jz}");
         qmb_dropin::PairTerms<T> pt(T_mat_in, J_dim_weights[0], J_dim_weights[2], 0);
         E_vecs = qmb_dropin::solve_irreps<T>(T_mat_in.GetLS(), GS_sector_in, SymmGroup_in, T_mat_in.GetR1(),
-                                             T_mat_in.GetR2(), pt.t, seed, tol_norm_in, NStates_in);
+                                             T_mat_in.GetR2(), pt.t, seed, tol_norm_in, NStates_in, &gs);
         seed_vecs.assign(E_vecs.size(), std::vector<long long>(1, seed));
     }
     virtual ~HeisenbergHamAbelianSymms_CUDA() {}
     std::vector<std::vector<float>> get_E_vecs() { return E_vecs; }
     std::vector<std::vector<long long>> get_seed_vecs() { return seed_vecs; }
+    // <GS|A|GS> in the lowest-energy irrep (HeisenbergHamAbelianSymms_CUDA.cu:448-617),
+    // on the kept ground state: no rebuild, no second Lanczos pass.
+    qmb_complex ComputeStaticExpValZeroT(ManyBodyOperator<qmb_complex> A, int max_terms = 0) {
+        (void)max_terms;
+        return qmb_dropin::expval(gs, A);
+    }
+    int get_GS_irrep() const { return gs.irrep; }
 
 protected:
     std::vector<std::vector<float>> E_vecs;
     std::vector<std::vector<long long>> seed_vecs;
+    qmb_dropin::GroundState gs;
 };
 
 // Generic XXZ model (Heisenberg<T>) in every irrep of G; GS_sector = -1 means L/2.
@@ -533,16 +896,24 @@ public:
         const int L = model.GetLS();
         const qmb_terms t = model.terms();
         E_vecs = qmb_dropin::solve_irreps<T>(L, GS_sector < 0 ? L / 2 : GS_sector, G, model.GetR1(), model.GetR2(), t,
-                                             seed, tol_norm, NStates);
+                                             seed, tol_norm, NStates, &gs);
         seed_vecs.assign(E_vecs.size(), std::vector<long long>(1, seed));
     }
     virtual ~HeisenbergXXZAbelianSymms_CUDA() {}
     std::vector<std::vector<float>> get_E_vecs() { return E_vecs; }
     std::vector<std::vector<long long>> get_seed_vecs() { return seed_vecs; }
+    // <GS|A|GS> in the lowest-energy irrep (HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:421-601),
+    // on the kept ground state: no rebuild, no second Lanczos pass.
+    qmb_complex ComputeStaticExpValZeroT(ManyBodyOperator<qmb_complex> A, int max_terms = 0) {
+        (void)max_terms;
+        return qmb_dropin::expval(gs, A);
+    }
+    int get_GS_irrep() const { return gs.irrep; }
 
 protected:
     std::vector<std::vector<float>> E_vecs;
     std::vector<std::vector<long long>> seed_vecs;
+    qmb_dropin::GroundState gs;
 };
 
 // The whole Sz sector without symmetry (exact_diagonalization/HeisenbergHam_CUDA.cu).
@@ -588,6 +959,20 @@ float LanczosEigVals_CUDA(float* E_tmp, int NStates, const int NIter, int nobv, 
                                           exportKrylovVec ? eig_vec_Krylov_out : nullptr, checkEigState ? 1 : 0,
                                           &residual));
     return residual;
+}
+
+// LanczosEigenStateFromSeed (exact_diagonalization/lanczos.cu:31-104): the
+// ground state sum_n eig_vec_Krylov[n] phi_n of a LanczosEigVals_CUDA run,
+// regenerated from the same seed into final_eig_vec_ptr (device, nobv of T).
+template <typename T>
+void LanczosEigenStateFromSeed(long long seed, T* final_eig_vec_ptr, std::vector<float> eig_vec_Krylov, int nobv,
+                               int NIter, int max_terms, uint32_t* index_mat, T* vals_mat, short int* track_vec,
+                               int threads = 512) {
+    (void)threads;
+    if ((int)eig_vec_Krylov.size() < NIter) eig_vec_Krylov.resize(NIter, 0.0f);
+    qmb_dropin::check(qmb_eigvec_from_seed_ref(seed, (void*)final_eig_vec_ptr, eig_vec_Krylov.data(), NIter, nobv,
+                                               max_terms, index_mat, (const void*)vals_mat,
+                                               (const int16_t*)track_vec, sizeof(T) == 2 * sizeof(float) ? 1 : 0));
 }
 
 #endif  // QMB_QMBCUDA_HPP

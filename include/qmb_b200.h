@@ -309,6 +309,11 @@ QMB_API qmb_status qmb_lanczos(qmb_ham h, const qmb_lanczos_opts* opts, qmb_lanc
                        double* krylov_coeffs, int64_t n_coeffs);
 /* Copies the kept ground-state vector (FP64, complex if the matrix is). */
 QMB_API qmb_status qmb_ground_state(qmb_ham h, void* psi /* host */, int64_t n);
+/* Puts a vector (FP64, complex if the matrix is; host memory) on the handle
+ * as its kept ground state, the counterpart of qmb_ground_state: a vector
+ * saved from an earlier solve of the same sector irrep becomes the state of
+ * qmb_expval without a new solve. */
+QMB_API qmb_status qmb_set_ground_state(qmb_ham h, const void* psi /* host */, int64_t n);
 
 /* LanczosEigVals_CUDA (exact_diagonalization/lanczos.h:20-32) on a
  * caller-owned reference-layout ELL in device memory: FP32 values, fixed
@@ -345,6 +350,36 @@ QMB_API qmb_status qmb_lanczos_ref_ell_noalloc(float* E, int n_iter, int nobv, i
                                        const void* val_dev, const int16_t* track_dev,
                                        int is_complex, float* krylov_out, int check_eig_state,
                                        float* residual, void* stream);
+
+/* LanczosEigenStateFromSeed (exact_diagonalization/lanczos.cu:31-104): the
+ * ground state sum_j krylov[j] v_j of a finished qmb_lanczos_ref_ell solve,
+ * regenerated from the same seed on the same reference-layout ELL.  The
+ * Lanczos vectors are bit-identical to the solve's (same start, same
+ * kernels); psi_dev receives nobv floats (complex: interleaved pairs).
+ * krylov is the host array the solve wrote to krylov_out; trailing zeros
+ * (a solve that broke down early) shorten the regeneration. */
+QMB_API qmb_status qmb_eigvec_from_seed_ref(long long seed, void* psi_dev, const float* krylov, int n_iter,
+                                    int nobv, int max_terms, const uint32_t* ind_dev,
+                                    const void* val_dev, const int16_t* track_dev, int is_complex);
+
+/* ================================================================ observables
+ * Zero-temperature expectation values out[2k] + i out[2k+1] =
+ * <psi|A_k|psi> / <psi|psi> for n_ops operators on the handle's sector irrep.
+ * Each A_k is a sum of products of Sz, S+, S- (and I) in the table form of
+ * qmb_terms -- the form the reference's ComputeStaticExpValZeroT builds from a
+ * ManyBodyOperator (HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:434-455): every
+ * term's factors daggered (S+ <-> S-) in application order and its scalar
+ * conjugated.  Replaces ComputeStaticExpValZeroT's rebuild + eigenvector
+ * regeneration + ExpecValArbOperatorAbelianIrrepProjHeisenbergZeroT + reduce
+ * (HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:421-601, utils.cu:442-550).
+ *
+ * psi_dev: the state on the device (FP64; complex double if the handle is
+ * complex), or NULL for the ground state kept on the handle (qmb_lanczos with
+ * want_vector, or qmb_set_ground_state).  Terms whose S+ and S- counts differ
+ * change Sz and contribute zero.  Other operator codes are QMB_ERR_INVALID.
+ * All operators are evaluated in one pass of one kernel per shared-memory
+ * chunk of terms; sums are FP64 and deterministic. */
+QMB_API qmb_status qmb_expval(qmb_ham h, int n_ops, const qmb_terms* ops, const void* psi_dev, double* out);
 
 /* ============================================================== batches
  * Many coupling sets over many sectors of one model family:

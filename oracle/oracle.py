@@ -83,6 +83,10 @@ def lib():
         L.oc_spmv.argtypes = [C.c_int64, C.c_int, u32p, f64p, i16p, f64p, f64p]
         L.oc_start_vector.restype = None
         L.oc_start_vector.argtypes = [C.c_uint64, C.c_int64, f64p]
+        L.oc_expval_ref.restype = None
+        L.oc_expval_ref.argtypes = [C.c_int, C.c_int, u32p, C.c_int, C.c_int64, u64p, u32p, f64p,
+                                    C.c_int, C.c_int, f64p, C.c_double, C.c_int, C.c_int, i32p,
+                                    i32p, i32p, f64p, f64p, C.c_int, f64p]
         _lib = L
     return _lib
 
@@ -128,6 +132,11 @@ def ref():
         R.ref_spmv_kernel_complex.argtypes = [u32p, f32p, i16p, f32p, f32p, C.c_int, C.c_int]
         R.ref_init_random_vec.restype = None
         R.ref_init_random_vec.argtypes = [C.c_longlong, C.c_int, f32p]
+        for nm in ("ref_expval_real", "ref_expval_complex"):
+            f = getattr(R, nm)
+            f.restype = None
+            f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u32p, u32p, C.c_int, f32p, C.c_int,
+                          f32p, C.c_float, C.c_int, C.c_int, i32p, i32p, i32p, f32p, f32p, f32p]
         for nm in ("ref_tstandard_real", "ref_tstandard_complex"):
             f = getattr(R, nm)
             f.restype = C.c_int
@@ -429,3 +438,179 @@ def ground_energy_sparse(A) -> float:
         return ground_energy_dense(A)
     w = sla.eigsh(A, k=1, which="SA", tol=1e-14, maxiter=100000)[0]
     return float(w[0])
+
+
+# ------------------------------------------------------------ observables
+def table_from_factors(terms) -> Terms:
+    """(scalar, [(code, site), ...]) physical terms -> driver tables: factors
+    daggered in written order, scalar conjugated, as ComputeStaticExpValZeroT
+    builds them (exact_diagonalization/HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:
+    434-455).  Codes 0 Sz, 1 Sp, 2 Sm, 9 I."""
+    terms = list(terms)
+    C_ = max([len(f) for _, f in terms] + [1])
+    dag = {0: 0, 1: 2, 2: 1, 9: 9}
+    n_ops = np.zeros(len(terms), np.int32)
+    codes = np.zeros(len(terms) * C_, np.int32)
+    sites = np.zeros(len(terms) * C_, np.int32)
+    sc = np.zeros(len(terms), np.complex128)
+    for t, (s, f) in enumerate(terms):
+        n_ops[t] = len(f)
+        for j, (c, q) in enumerate(f):
+            codes[t * C_ + j] = dag[c]
+            sites[t * C_ + j] = q
+        sc[t] = np.conj(s)
+    return Terms(n_ops, codes, sites, sc, C_)
+
+
+def expval_ref_rule(sec: Sector, terms: Terms, alpha: int, phi, with_break: bool = True,
+                    tol_norm: float = 1e-5) -> complex:
+    """Restatement of ExpecValArbOperatorAbelianIrrepProjHeisenbergZeroT + the
+    driver's reduction (utils.cu:442-550; HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:
+    596-597) on phi over all R orbits.  with_break keeps the reference's exit
+    from the member loop when a factor annihilates a member."""
+    g = sec.group
+    chars = np.ascontiguousarray(g.chars.astype(np.complex128)).view(np.float64).ravel()
+    ph = np.ascontiguousarray(np.asarray(phi, np.complex128)).view(np.float64).ravel()
+    out = np.zeros(2)
+    lib().oc_expval_ref(g.L, g.G, np.ascontiguousarray(g.perm).ravel(), g.n_ext, sec.R, sec.reps,
+                        sec.orbit, np.ascontiguousarray(sec.norms.ravel()), sec.norms.shape[1], alpha,
+                        chars, tol_norm, terms.H, terms.n_col, terms.n_ops, terms.codes, terms.sites,
+                        np.ascontiguousarray(terms.scalar).view(np.float64), ph, 1 if with_break else 0, out)
+    return complex(out[0], out[1])
+
+
+def apply_table(L: int, k: int, terms: Terms):
+    """Matrix M[t, s] = <t| table |s> of the tables applied in order (the
+    daggered operator) on the Sz sector in rank order."""
+    states = enumerate_sector(L, k)
+    pos = {int(s): i for i, s in enumerate(states)}
+    M = np.zeros((len(states), len(states)), np.complex128)
+    for j, s0 in enumerate(states):
+        for h in range(terms.H):
+            t = int(s0)
+            c = complex(terms.scalar[h])
+            ok = True
+            for x in range(terms.n_ops[h]):
+                code = terms.codes[h * terms.n_col + x]
+                q = terms.sites[h * terms.n_col + x]
+                spin = (t >> q) & 1
+                if code == 2:
+                    if not spin:
+                        ok = False
+                        break
+                    t &= ~(1 << q)
+                elif code == 1:
+                    if spin:
+                        ok = False
+                        break
+                    t |= 1 << q
+                elif code == 0:
+                    c *= 0.5 if spin else -0.5
+            if ok and t in pos:
+                M[pos[t], j] += c
+    return M
+
+
+def dense_operator(L: int, k: int, terms: Terms) -> np.ndarray:
+    """The physical operator of driver-form tables on the Sz sector (rank
+    order): the tables apply A^dagger, so A = (applied matrix)^H."""
+    return apply_table(L, k, terms).conj().T
+
+
+def irrep_basis(group: Group, alpha: int, k: int) -> np.ndarray:
+    """Orthonormal basis (columns, Sz-sector coordinates in rank order) of the
+    irrep alpha: the range of P = (1/n_ext) sum_e conj(chi_alpha(e)) U_e,
+    U_e moving the spin at site q to perm[e][q] (spin-inverted for e >= G).
+    This is the subspace whose lowest energy the sector's irrep alpha gives."""
+    L, G = group.L, group.G
+    states = enumerate_sector(L, k)
+    pos = {int(s): i for i, s in enumerate(states)}
+    n = len(states)
+    P = np.zeros((n, n), np.complex128)
+    for e in range(group.n_ext):
+        c = np.conj(group.chars[alpha, e]) / group.n_ext
+        row = np.ascontiguousarray(group.perm[e % G])
+        for j, s0 in enumerate(states):
+            t = int(lib().oc_apply(int(s0), L, row, 1 if e >= G else 0))
+            if t in pos:
+                P[pos[t], j] += c
+    w, V = np.linalg.eigh(0.5 * (P + P.conj().T))
+    return V[:, w > 0.5]
+
+
+def irrep_ground_state(Hd: np.ndarray, B: np.ndarray):
+    """Lowest eigenpair of Hd restricted to span(B): (E0, psi, gap)."""
+    w, v = np.linalg.eigh(B.conj().T @ Hd @ B)
+    return float(w[0]), B @ v[:, 0], float(w[1] - w[0]) if len(w) > 1 else np.inf
+
+
+def sym_table(group: Group, terms) -> list:
+    """Group average (1/n_ext) sum_e U_e^-1 A U_e of physical factor terms:
+    sites mapped by perm[e % G], S+ <-> S- and Sz -> -Sz for e >= G."""
+    out = []
+    flip = {0: 0, 1: 2, 2: 1, 9: 9}
+    for e in range(group.n_ext):
+        p = group.perm[e % group.G]
+        z = e >= group.G
+        for s, f in terms:
+            sign = (-1) ** sum(1 for c, _ in f if c == 0) if z else 1
+            out.append((s * sign / group.n_ext, [((flip[c] if z else c), int(p[q])) for c, q in f]))
+    return out
+
+
+def expval_sym_rule(sec: Sector, terms, alpha: int, phi, tol_norm: float = 1e-5) -> complex:
+    """conj(phi^H M phi) / |phi|^2 with M the symmetric-basis matrix (Hamiltonian
+    rule, ell_terms) of the group-averaged operator; phi over active rows.
+    Terms with unequal numbers of S+ and S- leave the Sz sector and have zero
+    expectation; they are dropped before the table is built."""
+    terms = [(s, f) for s, f in terms
+             if sum(1 for c, _ in f if c == 1) == sum(1 for c, _ in f if c == 2)]
+    if not terms:
+        return 0j
+    tab = table_from_factors(sym_table(sec.group, terms))
+    rows = active_rows(sec, alpha, tol_norm)
+    W = max(2, int(tab.H) + 1)
+    rc, ind, val, tr = ell_terms(sec, tab, alpha, W, tol_norm)
+    assert rc >= 0
+    M = ell_to_csr(ind, val, tr, rows)
+    M = M.toarray() if hasattr(M, "toarray") else np.asarray(M)
+    phi = np.asarray(phi, np.complex128)
+    return complex(np.conj(phi.conj() @ M @ phi) / np.vdot(phi, phi).real)
+
+
+def ref_expval(sec: Sector, terms: Terms, alpha: int, phi_orbits, tol_norm: float = 1e-5) -> complex:
+    """The reference's kernel itself (oracle/_ref) on phi over all R orbits,
+    FP32 as in the reference.  The group must have no spin inversion."""
+    g = sec.group
+    assert not g.flip
+    L, G, k = g.L, g.G, sec.k
+    n_irr = g.chars.shape[0]
+    n = binom(L, k)
+    chars32 = np.ascontiguousarray(g.chars.astype(np.complex64)).view(np.float32).ravel()
+    reps = np.zeros(max(n, 1), np.uint32)
+    srs = np.zeros(max(n * G, 1), np.uint32)
+    norms = np.zeros(max(n * n_irr, 1), np.float32)
+    orbit = np.zeros(max(2 * n, 1), np.uint32)
+    perm = np.ascontiguousarray(g.perm).ravel()
+    R = ref().ref_build_srs_complex(L, k, G, perm, n_irr, chars32, reps, n, srs, norms, orbit)
+    assert R == sec.R
+    act = {0: 0, 1: 1, 2: -1}
+    C_ = terms.n_col
+    actions = np.zeros(terms.H * C_, np.int32)
+    sites = -np.ones(terms.H * C_, np.int32)
+    for h in range(terms.H):
+        for x in range(terms.n_ops[h]):
+            actions[h * C_ + x] = act[int(terms.codes[h * C_ + x])]
+            sites[h * C_ + x] = terms.sites[h * C_ + x]
+    sc = np.ascontiguousarray(terms.scalar.astype(np.complex64)).view(np.float32).ravel()
+    out = np.zeros(2, np.float32)
+    phi = np.asarray(phi_orbits)
+    if np.iscomplexobj(phi):
+        f = ref().ref_expval_complex
+        ph = np.ascontiguousarray(phi.astype(np.complex64)).view(np.float32).ravel()
+    else:
+        f = ref().ref_expval_real
+        ph = np.ascontiguousarray(phi.astype(np.float32))
+    f(L, k, G, R, srs[: R * G], orbit[: 2 * n], n_irr, chars32, alpha, norms[: R * n_irr], tol_norm,
+      terms.H, C_, terms.n_ops, actions, sites, sc, ph, out)
+    return complex(float(out[0]), float(out[1]))

@@ -374,3 +374,62 @@ void oc_start_vector(uint64_t seed, int64_t n, double* out) {
         out[i] = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
     }
 }
+
+/* Zero-temperature expectation value with the rule of
+ * ExpecValArbOperatorAbelianIrrepProjHeisenbergZeroT
+ * (exact_diagonalization/utils.cu:442-550), then the sum over rows and the
+ * division by the group size of ComputeStaticExpValZeroT
+ * (HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:596-597).  Tables as that driver
+ * builds them (:434-455): codes daggered (0 Sz, 1 Sp, 2 Sm, 9 I), scalars
+ * conjugated.  For every orbit row and term the factors are applied to each
+ * member g_e(rep) of the orbit; the target's orbit o and member index e' come
+ * from the orbit map, and the row gains
+ *     conj(phi_row) conj(coef * (N_o / N_row) * conj(chi(e)) * chi(e')) phi_o.
+ * phi is complex [R] over all orbits.  with_break = 1 keeps the reference's
+ * loop exit (a factor that annihilates one member ends the member loop of
+ * that term); 0 visits every member.  Code 9 (identity) is skipped here; the
+ * reference's decode map has no entry for it and applies it as Sz.
+ * out = complex sum / n_ext. */
+void oc_expval_ref(int L, int G, const uint32_t* perm, int n_ext, int64_t R, const uint64_t* reps,
+                   const uint32_t* orbit_indices, const double* norms, int n_irr, int alpha,
+                   const double* chars, double tol_norm, int n_terms, int n_col, const int* n_ops,
+                   const int* op_code, const int* op_site, const double* scalar,
+                   const double* phi /* complex [R] */, int with_break, double* out /* complex */) {
+    cplx acc = 0;
+    const double* ch = chars + (size_t)2 * alpha * n_ext;
+    for (int64_t id = 0; id < R; ++id) {
+        double cn = norms[id * n_irr + alpha];
+        if (cn < tol_norm) continue;
+        cplx pid = phi[2 * id] + I * phi[2 * id + 1];
+        for (int ai = 0; ai < n_terms; ++ai) {
+            for (int gi = 0; gi < n_ext; ++gi) {
+                uint64_t t = apply_ext(reps[id], L, G, perm, gi);
+                cplx coef = scalar[2 * ai] + I * scalar[2 * ai + 1];
+                int bad = 0;
+                for (int k = 0; k < n_ops[ai]; ++k) {
+                    int site = op_site[ai * n_col + k], code = op_code[ai * n_col + k];
+                    int spin = (int)(t >> site & 1ull);
+                    if (code == 2) { if (!spin) { bad = 1; break; } t &= ~(1ull << site); }
+                    else if (code == 1) { if (spin) { bad = 1; break; } t |= 1ull << site; }
+                    else if (code == 0) { coef *= 0.5 * (-1.0 + 2.0 * spin); }
+                }
+                if (bad) {
+                    if (with_break) break;
+                    continue;
+                }
+                uint64_t rk = oc_rank(t);
+                uint32_t o = orbit_indices[2 * rk];
+                uint32_t e2 = orbit_indices[2 * rk + 1];
+                double tn = norms[(int64_t)o * n_irr + alpha];
+                if (tn < tol_norm) continue;
+                cplx cg = conj(ch[2 * gi] + I * ch[2 * gi + 1]);
+                cplx ce = ch[2 * e2] + I * ch[2 * e2 + 1];
+                cplx val = conj(coef * (tn / cn) * cg * ce);
+                acc += conj(pid) * val * (phi[2 * o] + I * phi[2 * o + 1]);
+            }
+        }
+    }
+    acc /= (double)n_ext;
+    out[0] = creal(acc);
+    out[1] = cimag(acc);
+}

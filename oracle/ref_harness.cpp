@@ -292,3 +292,48 @@ extern "C" int ref_tstandard_complex(int N1, int N2, int M, const float* A, cons
                          inter, cap, ti, tj, reinterpret_cast<cf*>(tv), R1, R2);
 }
 
+
+/* ExpecValArbOperatorAbelianIrrepProjHeisenbergZeroT<S> over all R orbit rows
+ * (the launch of HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:574-594, 32
+ * threads a block), then the reduction and the division by G of :596-597 as
+ * a sequential complex<float> sum.  Operator tables in the driver's form
+ * (:434-455): per factor an action (0 Sz, -1 lowering, +1 raising) and a
+ * site (-1 in unused slots), scalars already conjugated.  chars is the
+ * complex character table [NIr][G]; phi has R entries of S. */
+template <class S>
+static void expval(int L, int k, int G, int R, const uint32_t* srs, const uint32_t* orbit, int NIr,
+                   const cf* chars, int alpha, const float* norms, float tol, int A_size, int A_col,
+                   const int* n_ops, const int* actions, const int* sites, const cf* scalars,
+                   const S* phi, float* out) {
+    std::vector<uint32_t> bas = basis(L, k);
+    std::vector<cf> a_exp(R, cf(0.0f, 0.0f));
+    launch(R, 32, [&] {
+        ExpecValArbOperatorAbelianIrrepProjHeisenbergZeroT<S>(
+            const_cast<cf*>(scalars), const_cast<int*>(actions), const_cast<int*>(sites),
+            const_cast<int*>(n_ops), A_col, R, const_cast<uint32_t*>(srs), G, k,
+            const_cast<uint32_t*>(orbit), const_cast<cf*>(chars), alpha, const_cast<float*>(norms), NIr,
+            tol, A_size, A_col, bas.data(), const_cast<S*>(phi), a_exp.data());
+    });
+    cf sum(0.0f, 0.0f);
+    for (const cf& v : a_exp) sum = sum + v;
+    sum = sum / (float)G;
+    out[0] = sum.real();
+    out[1] = sum.imag();
+}
+
+extern "C" void ref_expval_real(int L, int k, int G, int R, const uint32_t* srs, const uint32_t* orbit, int NIr,
+                                const float* chars_ri, int alpha, const float* norms, float tol, int A_size,
+                                int A_col, const int* n_ops, const int* actions, const int* sites,
+                                const float* scalars_ri, const float* phi, float* out) {
+    expval<float>(L, k, G, R, srs, orbit, NIr, reinterpret_cast<const cf*>(chars_ri), alpha, norms, tol, A_size,
+                  A_col, n_ops, actions, sites, reinterpret_cast<const cf*>(scalars_ri), phi, out);
+}
+
+extern "C" void ref_expval_complex(int L, int k, int G, int R, const uint32_t* srs, const uint32_t* orbit,
+                                   int NIr, const float* chars_ri, int alpha, const float* norms, float tol,
+                                   int A_size, int A_col, const int* n_ops, const int* actions,
+                                   const int* sites, const float* scalars_ri, const float* phi_ri, float* out) {
+    expval<cf>(L, k, G, R, srs, orbit, NIr, reinterpret_cast<const cf*>(chars_ri), alpha, norms, tol, A_size,
+               A_col, n_ops, actions, sites, reinterpret_cast<const cf*>(scalars_ri),
+               reinterpret_cast<const cf*>(phi_ri), out);
+}

@@ -132,6 +132,9 @@ SIGNATURES = {
     "qmb_lanczos_default_opts": (None, [P(LanczosOpts)]),
     "qmb_lanczos": (i32, [vp, P(LanczosOpts), P(LanczosResult), vp, i64]),
     "qmb_ground_state": (i32, [vp, vp, i64]),
+    "qmb_set_ground_state": (i32, [vp, vp, i64]),
+    "qmb_eigvec_from_seed_ref": (i32, [C.c_longlong, vp, vp, i32, i32, i32, vp, vp, vp, i32]),
+    "qmb_expval": (i32, [vp, i32, P(Terms), vp, vp]),
     "qmb_lanczos_ref_ell": (i32, [P(C.c_float), i32, i32, i32, C.c_longlong, vp, vp, vp, i32,
                                   vp, i32, P(C.c_float)]),
     "qmb_lanczos_ref_ell_noalloc": (i32, [P(C.c_float), i32, i32, i32, C.c_longlong, vp, vp, vp,

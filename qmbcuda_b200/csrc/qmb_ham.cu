@@ -272,6 +272,7 @@ extern "C" qmb_status qmb_ham_create(qmb_sector s, const qmb_terms* terms, int p
         h->sector = s;
         h->device = s->device;
         h->n = s->n_active;
+        h->irrep_gen = s->irrep_gen;
         h->prec = prec | QMB_PREC_FP64;  // FP64 values are always built first
         h->cplx = !s->is_real || terms_complex(terms);
         upload_terms(h.get(), terms, s->L);

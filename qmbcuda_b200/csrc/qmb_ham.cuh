@@ -65,15 +65,16 @@ struct RowGen {
 };
 
 
-// Enumerates the entries of the row whose source string is src (norm ns):
-// emit(orbit, value) for every off-diagonal entry, the diagonal is returned.
+// Enumerates the entries of the row whose source string is src (norm ns)
+// generated by terms h0 .. h1-1: emit(orbit, value) for every off-diagonal
+// entry, the diagonal is returned.
 // Rule of BuildHamiltonianXXZForAbelianGroup (exact_diagonalization/utils.cu:83-184).
 template <class Emit>
-__device__ __forceinline__ double2 gen_row(const RowGen& rg, const GroupSmem& gs,
-                                           const TermsSmem& ts, uint64_t src, double ns,
-                                           Emit&& emit) {
+__device__ __forceinline__ double2 gen_row_range(const RowGen& rg, const GroupSmem& gs,
+                                                 const TermsSmem& ts, int h0, int h1, uint64_t src,
+                                                 double ns, Emit&& emit) {
     double2 diag = make_double2(0.0, 0.0);
-    for (int hi = 0; hi < ts.n_terms; ++hi) {
+    for (int hi = h0; hi < h1; ++hi) {
         uint64_t t = src;
         double2 coef = ts.scalar[hi];
         bool bad = false;
@@ -120,6 +121,14 @@ __device__ __forceinline__ double2 gen_row(const RowGen& rg, const GroupSmem& gs
         emit(o, v);
     }
     return diag;
+}
+
+// All terms of the table.
+template <class Emit>
+__device__ __forceinline__ double2 gen_row(const RowGen& rg, const GroupSmem& gs,
+                                           const TermsSmem& ts, uint64_t src, double ns,
+                                           Emit&& emit) {
+    return gen_row_range(rg, gs, ts, 0, ts.n_terms, src, ns, static_cast<Emit&&>(emit));
 }
 
 // --------------------------------------------------------- stored operator
@@ -271,6 +280,7 @@ struct MfOp {
 // Hamiltonian handle.
 struct qmb_ham_s {
     qmb_sector sector = nullptr;
+    int irrep_gen = 0;  // the sector irrep the handle was built for
     int device = 0;
     int64_t n = 0;
     bool cplx = false;

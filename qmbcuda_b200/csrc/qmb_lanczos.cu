@@ -751,6 +751,60 @@ extern "C" qmb_status qmb_ground_state(qmb_ham h, void* psi, int64_t n) {
     });
 }
 
+extern "C" qmb_status qmb_set_ground_state(qmb_ham h, const void* psi, int64_t n) {
+    return guarded([&] {
+        QMB_REQUIRE(h && psi, QMB_ERR_INVALID, "null argument");
+        QMB_REQUIRE(n == h->n, QMB_ERR_INVALID, "length differs from the handle's row count");
+        DeviceGuard dg(h->device);
+        const size_t bytes = (size_t)n * (h->cplx ? sizeof(double2) : sizeof(double));
+        h->psi.alloc(bytes);
+        QMB_CUDA_TRY(cudaMemcpy(h->psi.p, psi, bytes, cudaMemcpyHostToDevice));
+        h->psi_n = n;
+    });
+}
+
+// LanczosEigenStateFromSeed (exact_diagonalization/lanczos.cu:31-104): the
+// Lanczos vectors of qmb_lanczos_ref_ell are regenerated from the same cuRAND
+// start with the same kernels, so they are bit-identical to the solve's, and
+// psi = sum_j c_j v_j accumulates in the caller's FP32 type.  Trailing zero
+// coefficients (a solve that broke down early) end the regeneration there.
+extern "C" qmb_status qmb_eigvec_from_seed_ref(long long seed, void* psi_dev, const float* krylov, int n_iter,
+                                               int nobv, int max_terms, const uint32_t* ind_dev,
+                                               const void* val_dev, const int16_t* track_dev, int is_complex) {
+    return guarded([&] {
+        QMB_REQUIRE(psi_dev && krylov && ind_dev && val_dev && track_dev, QMB_ERR_INVALID, "null argument");
+        QMB_REQUIRE(nobv >= 1 && max_terms >= 1 && n_iter >= 1 && n_iter <= 4096, QMB_ERR_INVALID, "bad sizes");
+        int m = n_iter;
+        while (m > 0 && krylov[m - 1] == 0.0f) --m;
+        cudaStream_t s;
+        QMB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        struct SG { cudaStream_t s; ~SG() { cudaStreamDestroy(s); } } sg{s};
+        const size_t es = is_complex ? sizeof(float2) : sizeof(float);
+        QMB_CUDA_TRY(cudaMemsetAsync(psi_dev, 0, es * (size_t)nobv, s));
+        if (m == 0) {
+            QMB_CUDA_TRY(cudaStreamSynchronize(s));
+            return;
+        }
+        PhaseOut ph;
+        ph.m = m;
+        ph.s.assign(krylov, krylov + m);
+        LzState st;
+        st.init(m, lz_blocks(), false);
+        int n_hv = 0;
+        if (is_complex) {
+            RefEllOp<float2> op{nobv, max_terms, ind_dev, (const float2*)val_dev, track_dev};
+            DevBuf<float2> vr(2 * (size_t)nobv), wb(2 * (size_t)nobv);
+            ritz_vector<RefEllOp<float2>, float2, float2>(op, 0, ph, QMB_START_CURAND, (uint64_t)seed, nullptr,
+                                                          false, vr, 2, wb, st, (float2*)psi_dev, n_hv, s);
+        } else {
+            RefEllOp<float> op{nobv, max_terms, ind_dev, (const float*)val_dev, track_dev};
+            DevBuf<float> vr(2 * (size_t)nobv), wb(2 * (size_t)nobv);
+            ritz_vector<RefEllOp<float>, float, float>(op, 0, ph, QMB_START_CURAND, (uint64_t)seed, nullptr,
+                                                       false, vr, 2, wb, st, (float*)psi_dev, n_hv, s);
+        }
+    });
+}
+
 extern "C" qmb_status qmb_lanczos_ref_ell(float* E, int n_iter, int nobv, int max_terms,
                                           long long seed, const uint32_t* ind_dev,
                                           const void* val_dev, const int16_t* track_dev,

@@ -396,6 +396,7 @@ extern "C" qmb_status qmb_sector_set_irrep(qmb_sector s, const double* chars, do
         check_launch("k_active_maps");
         QMB_CUDA_TRY(cudaDeviceSynchronize());
         s->has_irrep = true;
+        ++s->irrep_gen;
     });
 }
 

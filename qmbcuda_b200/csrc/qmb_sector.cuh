@@ -23,6 +23,7 @@ struct qmb_sector_s {
 
     // selected irrep
     bool has_irrep = false;
+    int irrep_gen = 0;  // counts qmb_sector_set_irrep calls
     bool is_real = true;
     double tol_norm = 1e-5;
     std::vector<std::complex<double>> chars;  // [n_ext]

@@ -74,6 +74,66 @@ def xxz_terms(bonds, Jxy, Jz, part: str = "all") -> TermTable:
     return TermTable(np.array(n_ops), np.array(codes), np.array(sites), np.array(sc))
 
 
+_OP_CODE = {"Sz": A.OP_SZ, "Sp": A.OP_SP, "Sm": A.OP_SM, "I": A.OP_I}
+_DAGGER = {A.OP_SZ: A.OP_SZ, A.OP_SP: A.OP_SM, A.OP_SM: A.OP_SP, A.OP_I: A.OP_I}
+
+
+def operator_terms(terms) -> TermTable:
+    """A physical operator sum_t s_t O_t1 O_t2 ... O_tk as GPU-layer tables.
+
+    terms: iterable of (scalar, [(kind, site), ...]) with kind "Sz", "Sp",
+    "Sm" or "I" (or the QMB_OP_* codes), factors in written order.  Each
+    table row holds the factors daggered, in written order, and the conjugated
+    product of scalars: the tables ComputeStaticExpValZeroT builds from a
+    ManyBodyOperator (exact_diagonalization/
+    HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:434-455)."""
+    terms = list(terms)
+    width = max([len(f) for _, f in terms] + [1])
+    n_ops = np.zeros(len(terms), np.int32)
+    codes = np.zeros((len(terms), width), np.int32)
+    sites = np.zeros((len(terms), width), np.int32)
+    sc = np.zeros(len(terms), np.complex128)
+    for t, (s, factors) in enumerate(terms):
+        n_ops[t] = len(factors)
+        for j, (kind, site) in enumerate(factors):
+            codes[t, j] = _DAGGER[_OP_CODE[kind] if isinstance(kind, str) else int(kind)]
+            sites[t, j] = site
+        sc[t] = np.conj(s)
+    return TermTable(n_ops, codes, sites, sc)
+
+
+def fourier_terms(kind: str, k, N1: int, N2: int, a=(1.0, 0.0, 0.0, 1.0), n_sub: int = 1, alpha: int = 0,
+                  sign: int = 1):
+    """Factors of the Fourier operator O_k = N^-1/2 sum_cells e^{i k.r} O(site),
+    r = i a1 + j a2, site = (i N2 + j) n_sub + alpha, as FourierOperator
+    (quantum_operators/ArbitraryOperator.cu:246-282); sign=-1 gives O_{-k}.
+    Returns [(scalar, [(kind, site)])] for operator_terms or products."""
+    a1 = np.array([a[0], a[2]])
+    a2 = np.array([a[1], a[3]])
+    kk = sign * np.asarray(k, np.float64)
+    out = []
+    for i in range(N1):
+        for j in range(N2):
+            r = i * a1 + j * a2
+            out.append((np.exp(1j * float(kk @ r)) / np.sqrt(N1 * N2), [(kind, (i * N2 + j) * n_sub + alpha)]))
+    return out
+
+
+def multiply_terms(x, y):
+    """Product of two operators in (scalar, factors) form (factors of x first),
+    as ManyBodyOperator::operator* (ArbitraryOperator.cu:171-186)."""
+    return [(sa * sb, list(fa) + list(fb)) for sa, fa in x for sb, fb in y]
+
+
+def reciprocal_basis(a=(1.0, 0.0, 0.0, 1.0)):
+    """The matrix of ReciprocalBasisVectors (geometry/base.cpp:7-16) for
+    A_mat given row-major as a: its columns are b1, b2 with
+    a_i . b_j = 2 pi delta_ij (FullFourierOperator's k uses the columns)."""
+    det = a[0] * a[3] - a[1] * a[2]
+    c = 2.0 * np.pi / det
+    return np.array([[c * a[3], -c * a[2]], [-c * a[1], c * a[0]]])
+
+
 def chain_bonds(L: int, r: int = 1):
     return [(i, (i + r) % L) for i in range(L)]
 
@@ -263,6 +323,23 @@ class Hamiltonian:
         out = np.zeros(n, self.dtype(A.PREC_FP64))
         check(lib().qmb_ground_state(self.h, ptr(out), n))
         return out
+
+    def set_ground_state(self, psi) -> None:
+        psi = np.ascontiguousarray(psi, self.dtype(A.PREC_FP64))
+        check(lib().qmb_set_ground_state(self.h, ptr(psi), psi.shape[0]))
+
+    def expval(self, ops, psi_dev: int = 0) -> np.ndarray:
+        """<psi|A_k|psi> / <psi|psi> for each TermTable A_k (operator_terms
+        form) on the kept ground state, or on the device vector psi_dev."""
+        single = isinstance(ops, TermTable)
+        ops = [ops] if single else list(ops)
+        arr = (A.Terms * max(len(ops), 1))()
+        for k, t in enumerate(ops):
+            arr[k] = t.c()
+        out = np.zeros(2 * max(len(ops), 1))
+        check(lib().qmb_expval(self.h, len(ops), arr, C.c_void_p(psi_dev) if psi_dev else None, ptr(out)))
+        v = out[: 2 * len(ops)].view(np.complex128)
+        return v[0] if single else v
 
 
 class Batch:

@@ -10,7 +10,11 @@
 //  4. Heisenberg model with +-x Jxy rows of J/2 and Jz = J: physical chain
 //     energy -5.3873909174 from HeisenbergXXZAbelianSymms_CUDA.
 //  5. LanczosEigVals_CUDA on a reference-layout ELL (k=0 irrep) agrees with
-//     the k=0 energy of check 4 within FP32, 120 fixed steps.
+//     the k=0 energy of check 4 within FP32, 120 fixed steps; the state that
+//     LanczosEigenStateFromSeed regenerates has that energy.
+//  6. ComputeStaticExpValZeroT on the kept ground states of checks 1 and 4:
+//     <Sz0 Sz1> = E/(3L), <Sz0 Sz3>, <S+0 S-1> = 2 <Sz0 Sz1> and the structure
+//     factor at k = pi from FullFourierOperator, against dense FP64 values.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -84,6 +88,21 @@ static int run() {
     const std::vector<std::vector<float>> Ex = xxz.get_E_vecs();
     expect("heisenberg_model", lowest(Ex), -5.3873909174, 2e-6);
 
+    // 6. expectation values on the kept ground states
+    Sz<qmb_complex> sz0(0), sz1(1), sz3(3);
+    Sp<qmb_complex> sp0(0);
+    Sm<qmb_complex> sm1(1);
+    expect("expval_SzSz01", xxz.ComputeStaticExpValZeroT(sz0 * sz1).real(), -0.1496497477, 1e-5);
+    expect("expval_SzSz03", xxz.ComputeStaticExpValZeroT(SzSz_correlator<qmb_complex>(0, 3)).real(), -0.0552739149,
+           1e-5);
+    expect("expval_SpSm01", xxz.ComputeStaticExpValZeroT(sp0 * sm1).real(), -0.2992994954, 1e-5);
+    expect("expval_tstandard_SzSz01", Ham.ComputeStaticExpValZeroT(sz0 * sz1).real(), -0.1496497477, 1e-5);
+    auto Sk = FullFourierOperator(Sz<qmb_complex>(0), chain, false);
+    auto Skn = FullFourierOperator(Sz<qmb_complex>(0), chain, true);
+    const qmb_complex s_pi = xxz.ComputeStaticExpValZeroT(Sk[L / 2][0][0] * Skn[L / 2][0][0]);
+    expect("structure_factor_pi", s_pi.real(), 0.9829086368, 1e-5);
+    expect("structure_factor_pi_imag", s_pi.imag(), 0.0, 1e-6);
+
     // 5. LanczosEigVals_CUDA on the k = 0 reference-layout ELL
     std::vector<uint32_t> perm((size_t)L * L);
     T.GetGroupElemArr(model.GetR1(), model.GetR2(), perm.data());
@@ -118,6 +137,23 @@ static int run() {
     float E = 0.0f;
     std::vector<float> kry(120);
     const float res = LanczosEigVals_CUDA<float>(&E, 1, 120, R, W, 2212456, dind, dval, dtr, kry.data(), true, true);
+    float* dpsi = nullptr;
+    if (cudaMalloc(&dpsi, (size_t)R * 4) != cudaSuccess) {
+        std::printf("cudaMalloc failed\n");
+        return 2;
+    }
+    LanczosEigenStateFromSeed<float>(2212456, dpsi, kry, R, 120, W, dind, dval, dtr);
+    std::vector<float> psi(R);
+    cudaMemcpy(psi.data(), dpsi, (size_t)R * 4, cudaMemcpyDeviceToHost);
+    cudaFree(dpsi);
+    double num = 0.0, den = 0.0;
+    for (int r = 0; r < R; ++r) {
+        double y = 0.0;
+        for (int j = 0; j < track[r]; ++j) y += (double)valf[(size_t)r * W + j] * psi[ind[(size_t)r * W + j]];
+        num += psi[r] * y;
+        den += (double)psi[r] * psi[r];
+    }
+    expect("eigenstate_from_seed_energy", num / den, E, 1e-5);
     cudaFree(dind);
     cudaFree(dval);
     cudaFree(dtr);

@@ -19,6 +19,10 @@ Contents (key prefix = case):
                                   k=0 ELL (Heisenberg chain) and a seeded x
   e0_chain12                      dense FP64 ground energies of the 12 momentum
                                   irreps of the L=12 Heisenberg chain (oracle)
+  ev_chain10_a<a>_phi             FP32 ground state over all orbits of irrep a of
+                                  the L=10 Heisenberg chain (oracle ELL, dense)
+  ev_chain10_a<a>_<op>            ExpecValArbOperatorAbelianIrrepProjHeisenbergZeroT
+                                  + reduction / G on that state, operators EV_OPS
 """
 import os
 import sys
@@ -34,6 +38,34 @@ CASES = [("chain10", lambda: O.translation_group(10), 5, "chain"),
          ("square2x4", lambda: O.translation_group(2, 4), 4, "ring")]
 TSTD = [("chain16", 16, 1, 1, (1.0, 0.0, 0.0, 1.0), [1.0], [1.0001], 1, 1),
         ("square2x4_pbc", 2, 4, 1, (1.0, 0.0, 0.0, 1.0), [1.0, 0.15 + 0.15j], [1.0001, 1.4143], 1, 1)]
+
+
+# Operators of the expectation-value fixtures: (scalar, [(code, site), ...])
+# with codes 0 Sz, 1 Sp, 2 Sm, factors in written order.
+EV_OPS = {
+    "SzSz03": [(1.0, [(0, 0), (0, 3)])],
+    "SzSz01i": [(1j, [(0, 0), (0, 1)])],
+    "Sz2": [(1.0, [(0, 2)])],
+    "SzSzSzSz": [(2.0, [(0, 0), (0, 1), (0, 4), (0, 7)])],
+    "SpSm01": [(1.0, [(1, 0), (2, 1)])],
+    "SpSm02hc": [(0.5, [(1, 0), (2, 2)]), (0.5, [(2, 0), (1, 2)])],
+}
+EV_IRREPS = (0, 5, 1, 3)
+
+
+def ev_state(sec, a):
+    """Lowest eigenvector of irrep a of the L=10 Heisenberg chain over all R
+    orbits (zero on null orbits), normalised, as FP32 complex."""
+    t = O.xxz_terms(O.chain_bonds(sec.group.L), 1.0, 1.0)
+    rows = O.active_rows(sec, a)
+    rc, ind, val, tr = O.ell_terms(sec, t, a, 2 * sec.group.L + 1)
+    M = O.ell_to_csr(ind, val, tr, rows)
+    M = M.toarray() if hasattr(M, "toarray") else np.asarray(M)
+    w, V = np.linalg.eigh(M)
+    v = V[:, 0] / V[np.argmax(np.abs(V[:, 0])), 0] * np.abs(V[:, 0]).max()
+    phi = np.zeros(sec.R, np.complex128)
+    phi[rows] = v / np.linalg.norm(v)
+    return phi.astype(np.complex64)
 
 
 def ref_srs(R, g, k):
@@ -105,6 +137,16 @@ def main():
         rows = O.active_rows(sec, a)
         e0.append(O.ground_energy_dense(O.ell_to_csr(ind, val, tr, rows)) if len(rows) else np.nan)
     out["e0_chain12"] = np.array(e0)
+    # expectation values through the reference's kernel
+    g = O.translation_group(10)
+    sec = O.build_sector(g, 5)
+    for a in EV_IRREPS:
+        phi = ev_state(sec, a)
+        out[f"ev_chain10_a{a}_phi"] = phi
+        real = not np.any(phi.imag)
+        for nm, terms in EV_OPS.items():
+            v = O.ref_expval(sec, O.table_from_factors(terms), a, phi.real if real else phi)
+            out[f"ev_chain10_a{a}_{nm}"] = np.complex64(v)
     path = os.path.join(HERE, "reference_tables.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(out), "arrays")

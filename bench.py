@@ -182,6 +182,89 @@ def single_sector_hv(torch, q, reps=10):
     return out
 
 
+def _averaged_sz_terms(ops_sites, L):
+    """Distinct terms after averaging Sz-product terms over the L chain
+    translations (factors on distinct sites ordered by site), per operator."""
+    out = []
+    for terms in ops_sites:
+        keys = set()
+        for sites in terms:
+            for t in range(L):
+                m = [(x + t) % L for x in sites]
+                keys.add(tuple(sorted(m)) if len(set(m)) == len(m) else tuple(m))
+        out.append(len(keys))
+    return out
+
+
+def observables(torch, q, reps=5):
+    """Ground-state expectation values (qmb_expval) on the L=24 Heisenberg
+    chain, k=0 (112,720 rows): the structure factor <Sz_q Sz_-q> at all 24 q
+    (Fourier operators) and the 24 correlators <Sz_0 Sz_j>, 48 operators in one
+    call.  Time of the whole call (host group averaging, chunk staging and the
+    kernels) from CUDA events on the default stream, where it launches, and
+    from the wall clock; work = rows x group-averaged terms.  Beside it the
+    reference's member-loop rule (oracle restatement, one host thread) on
+    <Sz_0 Sz_1> of the same state."""
+    import oracle as O
+    A = q._capi
+    L = 24
+    perm, ch = q.translation_group(L)
+    s = q.Sector(L, L // 2, perm).set_irrep(ch[0])
+    h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L), 1.0, 1.0), prec=A.PREC_FP64)
+    h.lanczos(mode=A.MODE_FP64, max_iter=300, tol=1e-12, want_vector=1, allow_unconverged=True)
+    b = q.reciprocal_basis()
+    ops, sites = [], []
+    for n in range(L):
+        kv = n * b[:, 0] / L
+        f = q.multiply_terms(q.fourier_terms("Sz", kv, L, 1), q.fourier_terms("Sz", kv, L, 1, sign=-1))
+        ops.append(q.operator_terms(f))
+        sites.append([[x for _, x in fac] for _, fac in f])
+    for j in range(L):
+        ops.append(q.operator_terms([(1.0, [("Sz", 0), ("Sz", j)])]))
+        sites.append([[0, j]])
+    n_terms = int(np.sum(_averaged_sz_terms(sites, L)))
+    rows = int(h.info.n_rows)
+    h.expval(ops)
+    st = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dev, wall = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(st)
+        v = h.expval(ops)
+        e1.record(st)
+        e1.synchronize()
+        wall.append((time.perf_counter() - t0) * 1e3)
+        dev.append(e0.elapsed_time(e1))
+    ms = float(np.median(dev))
+    corr = v[L:].real
+    # the reference's rule on one host thread: every orbit member, one term
+    g = O.Group(L, np.ascontiguousarray(perm, np.uint32), np.asarray(ch, np.complex128))
+    sec = O.build_sector(g, L // 2)
+    phi = np.zeros(sec.R, np.complex128)
+    phi[O.active_rows(sec, 0)] = h.ground_state()
+    tab = O.table_from_factors([(1.0, [(0, 0), (0, 1)])])
+    t0 = time.perf_counter()
+    v_cpu = O.expval_ref_rule(sec, tab, 0, phi, with_break=True)
+    cpu_s = time.perf_counter() - t0
+    evals = rows * n_terms
+    out = {"workload": "L=24 Heisenberg chain ground state, k=0 (%d rows): S(q) at 24 q + 24 <Sz_0 Sz_j>, "
+                       "48 operators, %d group-averaged terms" % (rows, n_terms),
+           "kernel": "k_expval (+ k_expval_sum)", "ms_call": ms, "ms_wall": float(np.median(wall)),
+           "row_term_evals_per_s": evals / (ms * 1e-3),
+           "S_pi": float(v[L // 2].real), "SzSz_01": float(corr[1]),
+           "SzSz_01_times_3L": float(3 * L * corr[1]),
+           "cpu_reference_rule": {"operator": "<Sz_0 Sz_1>", "value": float(v_cpu.real),
+                                  "row_member_term_evals": int(sec.R) * L, "s": cpu_s,
+                                  "row_member_term_evals_per_s": sec.R * L / cpu_s, "cores": 1,
+                                  "kind": "port"}}
+    h.close()
+    s.close()
+    return out
+
+
 def run_batched(args, torch, q, rank, world):
     A = q._capi
     L, n_sets = 20, 256
@@ -239,6 +322,7 @@ def run_batched(args, torch, q, rank, world):
             s.close()
     e2e_s = float(np.mean(e2e_t)) if e2e_t else float("nan")
     single = None if args.no_compare else single_sector_hv(torch, q)
+    obs = None if args.no_compare else observables(torch, q)
     out = {
         "workload": "batched: 256 XXZ chains L=20 periodic, Delta~U(0,2), J~U(0.5,1.5) "
                     "(mt19937-64 seed 20261203), all k=0..19 of Sz=0, mixed precision",
@@ -263,6 +347,7 @@ def run_batched(args, torch, q, rank, world):
                      "ms_fp64": [round(v, 4) for v in b.info.tune_ms_fp64],
                      "variants": "(unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4)"},
         "single_sector_hv": single,
+        "observables": obs,
         "ms_steps": [round(float(v), 2) for v in dev_ms],
         "iters_mixed": [int(r.iters_low), int(r.iters)], "iters_fp64": int(r64.iters),
         "E0_min": float(E_mix.min()),

@@ -265,6 +265,54 @@ def observables(torch, q, reps=5):
     return out
 
 
+def table_files(torch, q, reps=3):
+    """Table files (qmb_sector_save/load, qmb_ham_save/load) against building
+    from scratch: the L=32 J1-J2 chain sector (k=0, spin-inversion even;
+    enumeration of C(32,16) strings) and the L=28 J1-J2 sector with its FP32
+    matrix.  Wall times of the public calls (median of `reps` after one
+    untimed round), file sizes, and whether the loaded tables and products
+    are bit-identical to the built ones."""
+    import tempfile
+    A = q._capi
+
+    def timed(f):
+        f()
+        ts, r = [], None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = f()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), r
+
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for L, with_ham in ((32, False), (28, True)):
+            perm, ch = q.translation_group(L)
+            chars = q.with_spin_flip(ch[0], 1)
+            t_build, s = timed(lambda: q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(chars))
+            ps = os.path.join(d, f"L{L}.sector")
+            t_save, _ = timed(lambda: s.save(ps))
+            t_load, s2 = timed(lambda: q.Sector.load(ps))
+            rec = {"rows": int(s.info.n_active), "orbits": int(s.info.n_orbits),
+                   "sector_build_s": t_build, "sector_save_s": t_save, "sector_load_s": t_load,
+                   "sector_file_mb": os.path.getsize(ps) / 1e6,
+                   "sector_identical": bool(np.array_equal(s.reps(), s2.reps()))}
+            if with_ham:
+                J = [1.0] * L + [0.5] * L
+                terms = q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J)
+                t_hb, h = timed(lambda: q.Hamiltonian(s, terms, prec=A.PREC_FP32))
+                ph = os.path.join(d, f"L{L}.ham")
+                t_hs, _ = timed(lambda: h.save(ph))
+                t_hl, h2 = timed(lambda: q.Hamiltonian.load(s2, ph))
+                x = np.random.default_rng(0).standard_normal(int(h.info.n_rows)).astype(np.float32)
+                same = np.array_equal(h.hv_host(x, A.PREC_FP32), h2.hv_host(x, A.PREC_FP32))
+                rec.update({"ham_build_s": t_hb, "ham_save_s": t_hs, "ham_load_s": t_hl,
+                            "ham_file_mb": os.path.getsize(ph) / 1e6, "hv_identical": bool(same)})
+            out[f"L{L}_j1j2_k0_even"] = rec
+    return out
+
+
 def run_batched(args, torch, q, rank, world):
     A = q._capi
     L, n_sets = 20, 256
@@ -323,6 +371,7 @@ def run_batched(args, torch, q, rank, world):
     e2e_s = float(np.mean(e2e_t)) if e2e_t else float("nan")
     single = None if args.no_compare else single_sector_hv(torch, q)
     obs = None if args.no_compare else observables(torch, q)
+    files = None if args.no_compare else table_files(torch, q)
     out = {
         "workload": "batched: 256 XXZ chains L=20 periodic, Delta~U(0,2), J~U(0.5,1.5) "
                     "(mt19937-64 seed 20261203), all k=0..19 of Sz=0, mixed precision",
@@ -348,6 +397,7 @@ def run_batched(args, torch, q, rank, world):
                      "variants": "(unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4)"},
         "single_sector_hv": single,
         "observables": obs,
+        "table_files": files,
         "ms_steps": [round(float(v), 2) for v in dev_ms],
         "iters_mixed": [int(r.iters_low), int(r.iters)], "iters_fp64": int(r64.iters),
         "E0_min": float(E_mix.min()),

@@ -50,6 +50,8 @@ typedef int qmb_status;
 #define QMB_ERR_TIMEOUT 6       /* a bounded device wait gave up                  */
 #define QMB_ERR_UNSUPPORTED 7   /* valid request outside what this build handles  */
 #define QMB_ERR_NO_DEVICE 8     /* no CUDA device is visible                      */
+#define QMB_ERR_IO 9            /* a table file could not be opened, read or written */
+#define QMB_ERR_CORRUPT 10      /* a table file fails its checksums or layout checks */
 
 /* Operator codes: the values of OperatorType
  * (quantum_operators/SingleParticleOperators.h:4). */
@@ -361,6 +363,39 @@ QMB_API qmb_status qmb_lanczos_ref_ell_noalloc(float* E, int n_iter, int nobv, i
 QMB_API qmb_status qmb_eigvec_from_seed_ref(long long seed, void* psi_dev, const float* krylov, int n_iter,
                                     int nobv, int max_terms, const uint32_t* ind_dev,
                                     const void* val_dev, const int16_t* track_dev, int is_complex);
+
+/* ============================================================== table files
+ * Versioned binary files for reuse across runs, in place of the reference's
+ * raw float dumps (WriteArrayToFile, utils/print_funcs.cu:73-90, called for
+ * vals_mat.bin / ind_mat.bin at HeisenbergHamAbelianSymms_CUDA.cu:149-162),
+ * which store indices as floats and carry no sizes or version.  A file has a
+ * header (magic "QMBTABLE", format version, kind, kind-specific scalars), a
+ * section table and 64-byte aligned payloads, each with a 64-bit checksum.
+ * Files are written under a temporary name and renamed.  Errors:
+ * QMB_ERR_IO (open, read, write), QMB_ERR_CORRUPT (checksums, truncation,
+ * layout), QMB_ERR_UNSUPPORTED (newer format version or other byte order).
+ *
+ * qmb_sector_save / qmb_sector_load: group, representatives and the selected
+ * irrep.  Loading skips the enumeration of all C(L, n_up) strings; it checks
+ * that every stored representative is its orbit's minimum and recomputes the
+ * irrep's norms on the device. */
+QMB_API qmb_status qmb_sector_save(qmb_sector s, const char* path);
+QMB_API qmb_status qmb_sector_load(const char* path, int device, qmb_sector* out);
+/* qmb_ham_save / qmb_ham_load: the sliced-ELL matrix, its values in every
+ * stored precision and its term tables.  The file records the sector and
+ * irrep it was built for (group, representatives, characters, tolerance);
+ * loading into a different one is QMB_ERR_INVALID. */
+QMB_API qmb_status qmb_ham_save(qmb_ham h, const char* path);
+QMB_API qmb_status qmb_ham_load(qmb_sector s, const char* path, qmb_ham* out);
+/* Reference-layout ELL tables in host memory (ind [n_rows][width] uint32,
+ * val [n_rows][width] float or complex float, track [n_rows] int16), the
+ * tables LanczosEigVals_CUDA consumes.  qmb_ref_ell_load with all three
+ * buffers NULL only reports the sizes; otherwise cap_rows must cover n_rows.
+ * No GPU is needed for either call. */
+QMB_API qmb_status qmb_ref_ell_save(const char* path, int64_t n_rows, int width, const uint32_t* ind,
+                            const void* val, const int16_t* track, int is_complex);
+QMB_API qmb_status qmb_ref_ell_load(const char* path, int64_t* n_rows, int* width, int* is_complex,
+                            uint32_t* ind, void* val, int16_t* track, int64_t cap_rows);
 
 /* ================================================================ observables
  * Zero-temperature expectation values out[2k] + i out[2k+1] =

@@ -8,13 +8,13 @@ fails if it has not been built (`python qmbcuda_b200/build.py`).
 from . import _capi
 from ._capi import QMBError, check, lib
 from .engine import (Batch, Hamiltonian, Sector, TermTable, chain_bonds, export_nosym,
-                     export_ref, fourier_terms, geometry, multiply_terms, operator_terms,
-                     reciprocal_basis, square_bonds, translation_group, with_spin_flip,
-                     xxz_terms)
+                     export_ref, fourier_terms, geometry, load_ref_ell, multiply_terms, operator_terms,
+                     reciprocal_basis, save_ref_ell, square_bonds, translation_group,
+                     with_spin_flip, xxz_terms)
 
 lib()
 
 __all__ = ["Batch", "Hamiltonian", "QMBError", "Sector", "TermTable", "chain_bonds", "check",
-           "export_nosym", "export_ref", "fourier_terms", "geometry", "lib", "multiply_terms",
-           "operator_terms", "reciprocal_basis", "square_bonds", "translation_group",
+           "export_nosym", "export_ref", "fourier_terms", "geometry", "lib", "load_ref_ell", "multiply_terms",
+           "operator_terms", "reciprocal_basis", "save_ref_ell", "square_bonds", "translation_group",
            "with_spin_flip", "xxz_terms"]

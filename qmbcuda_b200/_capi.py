@@ -22,6 +22,8 @@ QMB_ERR_NOT_CONVERGED = 5
 QMB_ERR_TIMEOUT = 6
 QMB_ERR_UNSUPPORTED = 7
 QMB_ERR_NO_DEVICE = 8
+QMB_ERR_IO = 9
+QMB_ERR_CORRUPT = 10
 
 OP_SZ, OP_SP, OP_SM, OP_I = 0, 1, 2, 9
 PREC_FP64, PREC_FP32 = 1, 2
@@ -135,6 +137,12 @@ SIGNATURES = {
     "qmb_set_ground_state": (i32, [vp, vp, i64]),
     "qmb_eigvec_from_seed_ref": (i32, [C.c_longlong, vp, vp, i32, i32, i32, vp, vp, vp, i32]),
     "qmb_expval": (i32, [vp, i32, P(Terms), vp, vp]),
+    "qmb_sector_save": (i32, [vp, C.c_char_p]),
+    "qmb_sector_load": (i32, [C.c_char_p, i32, P(vp)]),
+    "qmb_ham_save": (i32, [vp, C.c_char_p]),
+    "qmb_ham_load": (i32, [vp, C.c_char_p, P(vp)]),
+    "qmb_ref_ell_save": (i32, [C.c_char_p, i64, i32, vp, vp, vp, i32]),
+    "qmb_ref_ell_load": (i32, [C.c_char_p, P(i64), P(i32), P(i32), vp, vp, vp, i64]),
     "qmb_lanczos_ref_ell": (i32, [P(C.c_float), i32, i32, i32, C.c_longlong, vp, vp, vp, i32,
                                   vp, i32, P(C.c_float)]),
     "qmb_lanczos_ref_ell_noalloc": (i32, [P(C.c_float), i32, i32, i32, C.c_longlong, vp, vp, vp,

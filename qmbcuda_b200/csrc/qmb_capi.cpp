@@ -33,6 +33,8 @@ extern "C" const char* qmb_status_string(qmb_status s) {
         case QMB_ERR_TIMEOUT: return "device wait timed out";
         case QMB_ERR_UNSUPPORTED: return "unsupported";
         case QMB_ERR_NO_DEVICE: return "no CUDA device";
+        case QMB_ERR_IO: return "file I/O error";
+        case QMB_ERR_CORRUPT: return "corrupt table file";
         default: return "unknown status";
     }
 }

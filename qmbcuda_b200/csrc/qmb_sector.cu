@@ -231,70 +231,140 @@ static bool detect_rotations(const std::vector<uint32_t>& perm, int L, int G, in
 
 using namespace qmb;
 
+namespace qmb {
+
+void sector_check_desc(const qmb_sector_desc* d) {
+    QMB_REQUIRE(d->L >= 1 && d->L <= 64, QMB_ERR_INVALID, "L must be in 1..64");
+    QMB_REQUIRE(d->n_up >= 0 && d->n_up <= d->L, QMB_ERR_INVALID, "n_up must be in 0..L");
+    QMB_REQUIRE(d->n_perm >= 1 && d->n_perm <= kMaxPerm, QMB_ERR_INVALID,
+                "n_perm must be in 1..512");
+    QMB_REQUIRE(d->perm, QMB_ERR_INVALID, "perm is null");
+    QMB_REQUIRE(!d->spin_flip || 2 * d->n_up == d->L, QMB_ERR_INVALID,
+                "spin inversion needs 2*n_up == L");
+    const int L = d->L, G = d->n_perm;
+    for (int g = 0; g < G; ++g) {
+        std::vector<int> seen(L, 0);
+        for (int q = 0; q < L; ++q) {
+            uint32_t v = d->perm[(size_t)g * L + q];
+            QMB_REQUIRE(v < (uint32_t)L && !seen[v], QMB_ERR_INVALID,
+                        "perm row " + std::to_string(g) + " is not a permutation of 0..L-1");
+            seen[v] = 1;
+        }
+    }
+}
+
+// Fields and group tables of a sector (everything but the representatives).
+void sector_setup(qmb_sector_s* s, const qmb_sector_desc* d) {
+    const int L = d->L, G = d->n_perm;
+    s->device = d->device;
+    s->L = L;
+    s->n_up = d->n_up;
+    s->G = G;
+    s->flip = d->spin_flip ? 1 : 0;
+    s->n_ext = G * (1 + s->flip);
+    s->perm.assign(d->perm, d->perm + (size_t)G * L);
+    s->n_states = (int64_t)host_binom(L, d->n_up);
+    QMB_REQUIRE(s->n_states > 0, QMB_ERR_INVALID, "empty sector");
+
+    // group: word rotations when possible, else nibble tables
+    std::vector<ElemRot> rots;
+    bool structured = false;
+    for (int W = L; W >= 1 && !structured; --W)
+        if (L % W == 0 && detect_rotations(s->perm, L, G, W, rots)) {
+            structured = true;
+            s->W = W;
+        }
+    s->structured = structured ? 1 : 0;
+    s->n_chunks = (L + 3) / 4;
+    if (structured) {
+        s->rot.alloc(G);
+        s->rot.upload(rots.data(), G);
+    }
+    std::vector<uint64_t> tab((size_t)G * s->n_chunks * 16, 0);
+    for (int g = 0; g < G; ++g)
+        for (int c = 0; c < s->n_chunks; ++c)
+            for (int v = 0; v < 16; ++v) {
+                uint64_t y = 0;
+                for (int b = 0; b < 4; ++b) {
+                    int q = 4 * c + b;
+                    if (q < L && (v >> b & 1)) y |= 1ull << s->perm[(size_t)g * L + q];
+                }
+                tab[((size_t)g * s->n_chunks + c) * 16 + v] = y;
+            }
+    s->tables.alloc(tab.size());
+    s->tables.upload(tab.data(), tab.size());
+}
+
+// Counts stored representatives that are not the minimum of their orbit.
+__global__ void k_check_reps(GroupArgs g, const uint64_t* __restrict__ reps, int64_t R,
+                             unsigned long long* __restrict__ bad) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    GroupSmem gs = load_group(g, smem);
+    unsigned long long nb = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int e;
+        if (orbit_min(g, gs, reps[i], &e) != reps[i]) ++nb;
+    }
+    if (nb) atomicAdd(bad, nb);
+}
+
+qmb_sector_s* sector_from_reps(const qmb_sector_desc* d, const uint64_t* reps, int64_t R) {
+    sector_check_desc(d);
+    DeviceGuard dg(d->device);
+    upload_binomials();
+    auto s = std::make_unique<qmb_sector_s>();
+    sector_setup(s.get(), d);
+    QMB_REQUIRE(R > 0 && R < (1ll << 32) && R <= s->n_states, QMB_ERR_INVALID,
+                "stored representative count out of range");
+    const uint64_t mask = d->L == 64 ? ~0ull : ((1ull << d->L) - 1);
+    for (int64_t i = 0; i < R; ++i) {
+        QMB_REQUIRE((reps[i] & ~mask) == 0 && __builtin_popcountll(reps[i]) == d->n_up, QMB_ERR_INVALID,
+                    "a stored representative is not in the sector");
+        QMB_REQUIRE(i == 0 || reps[i] > reps[i - 1], QMB_ERR_INVALID,
+                    "stored representatives are not strictly ascending");
+    }
+    s->R = R;
+    s->reps.alloc(R);
+    s->reps.upload(reps, R);
+    GroupArgs ga = s->group_args();
+    size_t gsm = group_smem_bytes(ga);
+    DevBuf<unsigned long long> bad(1);
+    bad.zero();
+    set_group_smem_attr((const void*)k_check_reps, gsm);
+    k_check_reps<<<grid_for(R, 256), 256, gsm>>>(ga, s->reps.p, R, bad.p);
+    check_launch("k_check_reps");
+    unsigned long long nb = 0;
+    QMB_CUDA_TRY(cudaMemcpy(&nb, bad.p, sizeof(nb), cudaMemcpyDeviceToHost));
+    QMB_REQUIRE(nb == 0, QMB_ERR_INVALID, "stored representatives are not orbit minima of this group");
+    sector_buckets(s.get());
+    return s.release();
+}
+
+// Lookup buckets on the top T bits of the rank space over s->reps.
+void sector_buckets(qmb_sector_s* s) {
+    const int L = s->L;
+    s->T = std::min(L, 24);
+    uint64_t n_b = 1ull << s->T;
+    s->bucket.alloc(n_b + 1);
+    k_bucket<<<grid_for((int64_t)n_b + 1, 256), 256>>>(s->reps.p, s->R, L - s->T, n_b, s->bucket.p);
+    check_launch("k_bucket");
+    QMB_CUDA_TRY(cudaDeviceSynchronize());
+}
+
+}  // namespace qmb
+
 extern "C" qmb_status qmb_sector_create(const qmb_sector_desc* d, qmb_sector* out) {
     return guarded([&] {
         QMB_REQUIRE(d && out, QMB_ERR_INVALID, "null argument");
         *out = nullptr;
-        QMB_REQUIRE(d->L >= 1 && d->L <= 64, QMB_ERR_INVALID, "L must be in 1..64");
-        QMB_REQUIRE(d->n_up >= 0 && d->n_up <= d->L, QMB_ERR_INVALID, "n_up must be in 0..L");
-        QMB_REQUIRE(d->n_perm >= 1 && d->n_perm <= kMaxPerm, QMB_ERR_INVALID,
-                    "n_perm must be in 1..512");
-        QMB_REQUIRE(d->perm, QMB_ERR_INVALID, "perm is null");
-        QMB_REQUIRE(!d->spin_flip || 2 * d->n_up == d->L, QMB_ERR_INVALID,
-                    "spin inversion needs 2*n_up == L");
-        const int L = d->L, G = d->n_perm;
-        for (int g = 0; g < G; ++g) {
-            std::vector<int> seen(L, 0);
-            for (int q = 0; q < L; ++q) {
-                uint32_t v = d->perm[(size_t)g * L + q];
-                QMB_REQUIRE(v < (uint32_t)L && !seen[v], QMB_ERR_INVALID,
-                            "perm row " + std::to_string(g) + " is not a permutation of 0..L-1");
-                seen[v] = 1;
-            }
-        }
+        sector_check_desc(d);
         DeviceGuard dg(d->device);
         upload_binomials();
         auto s = new qmb_sector_s();
         std::unique_ptr<qmb_sector_s> own(s);
-        s->device = d->device;
-        s->L = L;
-        s->n_up = d->n_up;
-        s->G = G;
-        s->flip = d->spin_flip ? 1 : 0;
-        s->n_ext = G * (1 + s->flip);
-        s->perm.assign(d->perm, d->perm + (size_t)G * L);
-        s->n_states = (int64_t)host_binom(L, d->n_up);
-        QMB_REQUIRE(s->n_states > 0, QMB_ERR_INVALID, "empty sector");
-
-        // group: word rotations when possible, else nibble tables
-        std::vector<ElemRot> rots;
-        bool structured = false;
-        for (int W = L; W >= 1 && !structured; --W)
-            if (L % W == 0 && detect_rotations(s->perm, L, G, W, rots)) {
-                structured = true;
-                s->W = W;
-            }
-        s->structured = structured ? 1 : 0;
-        s->n_chunks = (L + 3) / 4;
-        if (structured) {
-            s->rot.alloc(G);
-            s->rot.upload(rots.data(), G);
-        }
-        {
-            std::vector<uint64_t> tab((size_t)G * s->n_chunks * 16, 0);
-            for (int g = 0; g < G; ++g)
-                for (int c = 0; c < s->n_chunks; ++c)
-                    for (int v = 0; v < 16; ++v) {
-                        uint64_t y = 0;
-                        for (int b = 0; b < 4; ++b) {
-                            int q = 4 * c + b;
-                            if (q < L && (v >> b & 1)) y |= 1ull << s->perm[(size_t)g * L + q];
-                        }
-                        tab[((size_t)g * s->n_chunks + c) * 16 + v] = y;
-                    }
-            s->tables.alloc(tab.size());
-            s->tables.upload(tab.data(), tab.size());
-        }
+        sector_setup(s, d);
+        const int L = s->L;
         GroupArgs ga = s->group_args();
         size_t gsm = group_smem_bytes(ga);
 
@@ -321,15 +391,7 @@ extern "C" qmb_status qmb_sector_create(const qmb_sector_desc* d, qmb_sector* ou
         k_rep_write<<<grid_for((int64_t)n_words, 256), 256>>>(L, s->n_up, n_words, words.p,
                                                               offsets.p, s->reps.p);
         check_launch("k_rep_write");
-
-        // lookup buckets on the top T bits
-        s->T = std::min(L, 24);
-        uint64_t n_b = 1ull << s->T;
-        s->bucket.alloc(n_b + 1);
-        k_bucket<<<grid_for((int64_t)n_b + 1, 256), 256>>>(s->reps.p, s->R, L - s->T, n_b,
-                                                           s->bucket.p);
-        check_launch("k_bucket");
-        QMB_CUDA_TRY(cudaDeviceSynchronize());
+        sector_buckets(s);
         *out = own.release();
     });
 }
@@ -354,49 +416,56 @@ extern "C" qmb_status qmb_sector_get_info(qmb_sector s, qmb_sector_info* info) {
     });
 }
 
+namespace qmb {
+// Irrep selection: characters, norms and the active-row maps.
+void sector_select_irrep(qmb_sector_s* s, const double* chars, double tol_norm) {
+    s->chars.resize(s->n_ext);
+    s->is_real = true;
+    std::vector<double2> ch(s->n_ext);
+    for (int e = 0; e < s->n_ext; ++e) {
+        s->chars[e] = {chars[2 * e], chars[2 * e + 1]};
+        ch[e] = make_double2(chars[2 * e], chars[2 * e + 1]);
+        QMB_REQUIRE(std::isfinite(chars[2 * e]) && std::isfinite(chars[2 * e + 1]),
+                    QMB_ERR_INVALID, "non-finite character");
+        if (std::fabs(chars[2 * e + 1]) > 1e-12) s->is_real = false;
+    }
+    s->tol_norm = tol_norm;
+    s->chars_dev.alloc(s->n_ext);
+    s->chars_dev.upload(ch.data(), s->n_ext);
+    GroupArgs ga = s->group_args();
+    size_t gsm = group_smem_bytes(ga);
+    s->norms.alloc(s->R);
+    DevBuf<int> active(s->R + 1);
+    DevBuf<int64_t> pos(s->R + 1);
+    set_group_smem_attr((const void*)k_norms, gsm);
+    k_norms<<<grid_for(s->R, 256), 256, gsm>>>(ga, s->reps.p, s->R, tol_norm, s->norms.p,
+                                               active.p);
+    check_launch("k_norms");
+    QMB_CUDA_TRY(cudaMemsetAsync(active.p + s->R, 0, sizeof(int)));
+    size_t tmp_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, active.p, pos.p, s->R + 1);
+    DevBuf<unsigned char> tmp(tmp_bytes);
+    cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, active.p, pos.p, s->R + 1);
+    int64_t na = 0;
+    QMB_CUDA_TRY(cudaMemcpy(&na, pos.p + s->R, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    s->n_active = na;
+    s->row_of_orbit.alloc(s->R);
+    s->orbit_of_row.alloc(na > 0 ? na : 1);
+    k_active_maps<<<grid_for(s->R, 256), 256>>>(s->R, active.p, pos.p, s->row_of_orbit.p,
+                                                s->orbit_of_row.p);
+    check_launch("k_active_maps");
+    QMB_CUDA_TRY(cudaDeviceSynchronize());
+    s->has_irrep = true;
+    ++s->irrep_gen;
+}
+}  // namespace qmb
+
 extern "C" qmb_status qmb_sector_set_irrep(qmb_sector s, const double* chars, double tol_norm) {
     return guarded([&] {
         QMB_REQUIRE(s && chars, QMB_ERR_INVALID, "null argument");
         QMB_REQUIRE(tol_norm >= 0, QMB_ERR_INVALID, "tol_norm must be >= 0");
         DeviceGuard dg(s->device);
-        s->chars.resize(s->n_ext);
-        s->is_real = true;
-        std::vector<double2> ch(s->n_ext);
-        for (int e = 0; e < s->n_ext; ++e) {
-            s->chars[e] = {chars[2 * e], chars[2 * e + 1]};
-            ch[e] = make_double2(chars[2 * e], chars[2 * e + 1]);
-            QMB_REQUIRE(std::isfinite(chars[2 * e]) && std::isfinite(chars[2 * e + 1]),
-                        QMB_ERR_INVALID, "non-finite character");
-            if (std::fabs(chars[2 * e + 1]) > 1e-12) s->is_real = false;
-        }
-        s->tol_norm = tol_norm;
-        s->chars_dev.alloc(s->n_ext);
-        s->chars_dev.upload(ch.data(), s->n_ext);
-        GroupArgs ga = s->group_args();
-        size_t gsm = group_smem_bytes(ga);
-        s->norms.alloc(s->R);
-        DevBuf<int> active(s->R + 1);
-        DevBuf<int64_t> pos(s->R + 1);
-        set_group_smem_attr((const void*)k_norms, gsm);
-        k_norms<<<grid_for(s->R, 256), 256, gsm>>>(ga, s->reps.p, s->R, tol_norm, s->norms.p,
-                                                   active.p);
-        check_launch("k_norms");
-        QMB_CUDA_TRY(cudaMemsetAsync(active.p + s->R, 0, sizeof(int)));
-        size_t tmp_bytes = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, active.p, pos.p, s->R + 1);
-        DevBuf<unsigned char> tmp(tmp_bytes);
-        cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, active.p, pos.p, s->R + 1);
-        int64_t na = 0;
-        QMB_CUDA_TRY(cudaMemcpy(&na, pos.p + s->R, sizeof(int64_t), cudaMemcpyDeviceToHost));
-        s->n_active = na;
-        s->row_of_orbit.alloc(s->R);
-        s->orbit_of_row.alloc(na > 0 ? na : 1);
-        k_active_maps<<<grid_for(s->R, 256), 256>>>(s->R, active.p, pos.p, s->row_of_orbit.p,
-                                                    s->orbit_of_row.p);
-        check_launch("k_active_maps");
-        QMB_CUDA_TRY(cudaDeviceSynchronize());
-        s->has_irrep = true;
-        ++s->irrep_gen;
+        sector_select_irrep(s, chars, tol_norm);
     });
 }
 

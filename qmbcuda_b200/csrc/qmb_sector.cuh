@@ -24,6 +24,7 @@ struct qmb_sector_s {
     // selected irrep
     bool has_irrep = false;
     int irrep_gen = 0;  // counts qmb_sector_set_irrep calls
+    uint64_t reps_sum = 0;  // checksum of reps for table files (0: not computed yet)
     bool is_real = true;
     double tol_norm = 1e-5;
     std::vector<std::complex<double>> chars;  // [n_ext]
@@ -55,3 +56,18 @@ struct qmb_sector_s {
         return t;
     }
 };
+
+#include "qmb_b200.h"
+
+namespace qmb {
+// Pieces of qmb_sector_create / qmb_sector_set_irrep shared with the
+// table-file loader (qmb_store.cu).
+void sector_check_desc(const qmb_sector_desc* d);
+void sector_setup(qmb_sector_s* s, const qmb_sector_desc* d);
+void sector_buckets(qmb_sector_s* s);
+void sector_select_irrep(qmb_sector_s* s, const double* chars, double tol_norm);
+// A sector from stored representatives instead of an enumeration.  The
+// representatives are checked: ascending, in the sector, and each the
+// minimum of its orbit under the group.
+qmb_sector_s* sector_from_reps(const qmb_sector_desc* d, const uint64_t* reps, int64_t R);
+}  // namespace qmb

@@ -6,6 +6,7 @@ host buffers (or raw device pointers for the device-side entry points).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -188,6 +189,20 @@ class Sector:
         self.h = h
         self.L, self.n_up = L, n_up
 
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "Sector":
+        """A sector (and its saved irrep) from a table file of save()."""
+        h = C.c_void_p()
+        check(lib().qmb_sector_load(os.fsencode(path), device, C.byref(h)))
+        s = cls.__new__(cls)
+        s.h = h
+        s._perm = None
+        s.L = s.n_up = None
+        return s
+
+    def save(self, path: str) -> None:
+        check(lib().qmb_sector_save(self.h, os.fsencode(path)))
+
     def close(self):
         if getattr(self, "h", None):
             lib().qmb_sector_destroy(self.h)
@@ -263,6 +278,30 @@ def export_nosym(L: int, n_up: int, terms: TermTable, W: int, device: int = 0):
     return ind.reshape(n, W), val.view(np.complex128).reshape(n, W), track
 
 
+def save_ref_ell(path: str, ind, val, track) -> None:
+    """Reference-layout ELL tables (host arrays) to a table file."""
+    ind = np.ascontiguousarray(ind, np.uint32)
+    cplx = np.iscomplexobj(val)
+    val = np.ascontiguousarray(val, np.complex64 if cplx else np.float32)
+    track = np.ascontiguousarray(track, np.int16)
+    R, W = ind.shape
+    assert val.shape == (R, W) and track.shape == (R,)
+    check(lib().qmb_ref_ell_save(os.fsencode(path), R, W, ptr(ind), ptr(val), ptr(track), int(cplx)))
+
+
+def load_ref_ell(path: str):
+    """(ind, val, track) of a reference-layout ELL table file."""
+    R, W, cp = C.c_int64(), C.c_int(), C.c_int()
+    p = os.fsencode(path)
+    check(lib().qmb_ref_ell_load(p, C.byref(R), C.byref(W), C.byref(cp), None, None, None, 0))
+    ind = np.zeros((R.value, W.value), np.uint32)
+    val = np.zeros((R.value, W.value), np.complex64 if cp.value else np.float32)
+    track = np.zeros(R.value, np.int16)
+    check(lib().qmb_ref_ell_load(p, C.byref(R), C.byref(W), C.byref(cp), ptr(ind), ptr(val), ptr(track),
+                                 R.value))
+    return ind, val, track
+
+
 class Hamiltonian:
     """Matrix of a sector's irrep in sliced ELL on the device (qmb_ham)."""
 
@@ -273,6 +312,18 @@ class Hamiltonian:
         h = C.c_void_p()
         check(lib().qmb_ham_create(sector.h, C.byref(t), prec, C.byref(h)))
         self.h = h
+
+    @classmethod
+    def load(cls, sector: Sector, path: str) -> "Hamiltonian":
+        """A matrix from a table file of save(), on the sector irrep it was built for."""
+        h = C.c_void_p()
+        check(lib().qmb_ham_load(sector.h, os.fsencode(path), C.byref(h)))
+        m = cls.__new__(cls)
+        m.sector, m.terms, m.h = sector, None, h
+        return m
+
+    def save(self, path: str) -> None:
+        check(lib().qmb_ham_save(self.h, os.fsencode(path)))
 
     def close(self):
         if getattr(self, "h", None):

@@ -1068,23 +1068,29 @@ static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st
     cudaEvent_t e0, e1;
     QMB_CUDA_TRY(cudaEventCreate(&e0));
     QMB_CUDA_TRY(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int arg = 0;
+    // variants timed round-robin (five rounds, minimum per variant), so that
+    // clock ramp-up or a one-off delay does not decide the choice
+    float tmin[kBVariants];
     for (int c = 0; c < kBVariants; ++c) {
+        tmin[c] = 1e30f;
         bhv_variant<V>(c, a, k, x.p, y.p, nullptr, 1, lz, nullptr, nullptr, 0, st);  // warm
-        float tmin = 1e30f;
-        for (int r = 0; r < 3; ++r) {
+    }
+    for (int r = 0; r < 5; ++r)
+        for (int c = 0; c < kBVariants; ++c) {
             cudaEventRecord(e0, st);
             bhv_variant<V>(c, a, k, x.p, y.p, nullptr, 1, lz, nullptr, nullptr, 0, st);
             cudaEventRecord(e1, st);
             cudaEventSynchronize(e1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            tmin = std::min(tmin, ms);
+            tmin[c] = std::min(tmin[c], ms);
         }
-        k.tune_ms[f64 ? 1 : 0][c] = tmin;
-        if (tmin < best) {
-            best = tmin;
+    float best = 1e30f;
+    int arg = 0;
+    for (int c = 0; c < kBVariants; ++c) {
+        k.tune_ms[f64 ? 1 : 0][c] = tmin[c];
+        if (tmin[c] < best) {
+            best = tmin[c];
             arg = c;
         }
     }

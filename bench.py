@@ -315,8 +315,107 @@ def table_files(torch, q, reps=3):
     return out
 
 
+def single_sector_configs(torch, q):
+    """The single-sector configurations, each one solve or product on one GPU
+    (device times from the library's CUDA events; products from CUDA events
+    on the launch stream):
+      L=24 XXZ chain, Delta=0.5, k=0, spin-inversion even: FP64 vs mixed solve;
+      L=32 J1-J2 chain, k=0, even: stored and matrix-free products, FP64 solve
+        and mixed solves with two reorthogonalisation passes (stored and
+        matrix-free);
+      6x6 square lattice, k=(0,0), even: stored FP32 and matrix-free products."""
+    A = q._capi
+    st = torch.cuda.current_stream()
+
+    def t_hv(h, prec, mf, reps):
+        dt = torch.float64 if prec == A.PREC_FP64 else torch.float32
+        n = int(h.info.n_rows)
+        x = torch.randn(n, dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        f = q.lib().qmb_hv_matrix_free if mf else q.lib().qmb_hv
+        args = (h.h, prec, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), A.C.c_void_p(st.cuda_stream))
+        q.check(f(*args))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(reps):
+            q.check(f(*args))
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def solve(h, **kw):
+        h.lanczos(**kw)
+        r = h.lanczos(**kw)
+        return {"ms": r.ms_total, "products": int(r.n_hv), "hv_per_s": r.n_hv / (r.ms_total * 1e-3),
+                "iters": [int(r.iters_low), int(r.iters)], "E0": r.E0, "residual": r.residual}
+
+    peak, _ = load_peaks()
+    out = {}
+    L = 24
+    perm, ch = q.translation_group(L)
+    s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+    h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L), 1.0, 0.5))
+    f64 = solve(h, mode=A.MODE_FP64, tol=1e-12)
+    mix = solve(h, mode=A.MODE_MIXED, tol=1e-12)
+    out["L24_xxz_d0.5_k0_even"] = {"rows": int(h.info.n_rows), "fp64": f64, "mixed": mix,
+                                   "rel_dE0": abs(mix["E0"] - f64["E0"]) / abs(f64["E0"]),
+                                   "hv_us_fp64": 1e3 * t_hv(h, A.PREC_FP64, False, 50),
+                                   "hv_us_fp32": 1e3 * t_hv(h, A.PREC_FP32, False, 50)}
+    h.close()
+    s.close()
+    L = 32
+    perm, ch = q.translation_group(L)
+    s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+    J = [1.0] * L + [0.5] * L
+    h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J))
+    i = h.info
+    ms64, ms32 = t_hv(h, A.PREC_FP64, False, 10), t_hv(h, A.PREC_FP32, False, 10)
+    mf32 = t_hv(h, A.PREC_FP32, True, 3)
+    f64 = solve(h, mode=A.MODE_FP64, tol=1e-12, max_iter=300)
+    mix = solve(h, mode=A.MODE_MIXED, tol=1e-12, max_iter=300, reorth=2)
+    r = h.lanczos(mode=A.MODE_MIXED, tol=1e-12, max_iter=300, reorth=2, hv=A.HV_MATRIX_FREE)
+    out["L32_j1j2_k0_even"] = {
+        "rows": int(i.n_rows), "nnz": int(i.nnz_offdiag),
+        "hv_ms_fp64": ms64, "hv_gbs_fp64": i.bytes_fp64 / (ms64 * 1e-3) / 1e9,
+        "hv_frac_fp64": i.bytes_fp64 / (ms64 * 1e-3) / 1e9 / peak,
+        "hv_ms_fp32": ms32, "hv_gbs_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9,
+        "hv_frac_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9 / peak,
+        "hv_ms_matrix_free_fp32": mf32,
+        "fp64": f64, "mixed_reorth2": mix, "rel_dE0": abs(mix["E0"] - f64["E0"]) / abs(f64["E0"]),
+        "mixed_reorth2_matrix_free": {"ms": r.ms_total, "products": int(r.n_hv),
+                                      "rel_dE0": abs(r.E0 - f64["E0"]) / abs(f64["E0"])}}
+    h.close()
+    s.close()
+    N = 6
+    perm, ch = q.translation_group(N, N)
+    t0 = time.perf_counter()
+    s = q.Sector(N * N, N * N // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+    t_sec = time.perf_counter() - t0
+    h = q.Hamiltonian(s, q.xxz_terms(q.square_bonds(N, N), 1.0, 1.0), prec=A.PREC_FP32)
+    t_ham = time.perf_counter() - t0 - t_sec
+    i = h.info
+    ms32 = t_hv(h, A.PREC_FP32, False, 5)
+    mf32 = t_hv(h, A.PREC_FP32, True, 2)
+    gathers = float(i.nnz_offdiag) * 32.0  # one 32-byte DRAM sector per gathered x element
+    out["6x6_k00_even"] = {
+        "rows": int(i.n_rows), "nnz": int(i.nnz_offdiag), "sector_build_s": t_sec, "ham_build_s": t_ham,
+        "hv_ms_fp32": ms32, "hv_gbs_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9,
+        "hv_frac_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9 / peak,
+        "hv_sector_gbs_fp32": gathers / (ms32 * 1e-3) / 1e9,
+        "hv_ms_matrix_free_fp32": mf32}
+    h.close()
+    s.close()
+    return out
+
+
 def run_batched(args, torch, q, rank, world):
     A = q._capi
+    # the single-sector configurations first, while the device memory is free
+    # (the 6x6 matrix needs ~100 GB while it is built)
+    configs = None if args.no_compare else single_sector_configs(torch, q)
+    torch.cuda.empty_cache()
     L, n_sets = 20, 256
     J, D = couplings(n_sets, rank)
     secs, b = build_batched(q, L, n_sets)
@@ -416,6 +515,7 @@ def run_batched(args, torch, q, rank, world):
         "single_sector_hv": single,
         "observables": obs,
         "table_files": files,
+        "single_sector_configs": configs,
         "ms_steps": [round(float(v), 2) for v in dev_ms],
         "iters_mixed": [int(r.iters_low), int(r.iters)], "iters_fp64": int(r64.iters),
         "E0_min": float(E_mix.min()),

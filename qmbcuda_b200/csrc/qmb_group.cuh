@@ -83,8 +83,37 @@ __device__ __forceinline__ uint64_t apply_elem(const GroupArgs& g, const GroupSm
     return z ? (y ^ g.mask) : y;
 }
 
+// Structured groups on at most 32 sites: the same site maps in 32-bit
+// arithmetic (a 64-bit shift, mask or compare costs several 32-bit ALU
+// instructions, and the orbit search is ALU-bound).  Same loop order and
+// comparisons as the 64-bit forms, so the same element is chosen.
+__device__ __forceinline__ uint32_t rot32_bits(uint32_t x, int r, int L, uint32_t mask) {
+    if (r == 0) return x;
+    return ((x << r) | (x >> (L - r))) & mask;
+}
+
+__device__ __forceinline__ uint32_t rot32_rows(uint32_t x, int c, int W, uint32_t lo) {
+    if (c == 0) return x;
+    return ((x & lo) << c) | ((x & ~lo) >> (W - c));
+}
+
+__device__ __forceinline__ uint32_t apply_site_map32(const GroupArgs& g, const GroupSmem& sm, int gi, uint32_t s) {
+    const ElemRot e = sm.rot[gi];
+    return rot32_rows(rot32_bits(s, (int)e.rr, g.L, (uint32_t)g.mask), (int)e.ri, g.W, (uint32_t)e.lo);
+}
+
 // True iff no element maps s below s (s is its orbit's minimum).
 __device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, uint64_t s) {
+    if (g.structured && g.L <= 32) {
+        const uint32_t x = (uint32_t)s, m = (uint32_t)g.mask;
+        const bool flip = g.n_ext > g.G;
+        for (int gi = 0; gi < g.G; ++gi) {
+            const uint32_t y = apply_site_map32(g, sm, gi, x);
+            if (y < x) return false;
+            if (flip && (y ^ m) < x) return false;
+        }
+        return true;
+    }
     for (int gi = 0; gi < g.G; ++gi) {
         uint64_t y = apply_site_map(g, sm, gi, s);
         if (y < s) return false;
@@ -96,6 +125,26 @@ __device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, 
 // Minimum of the orbit of t and the first element reaching it.
 __device__ __forceinline__ uint64_t orbit_min(const GroupArgs& g, const GroupSmem& sm, uint64_t t,
                                               int* elem) {
+    if (g.structured && g.L <= 32) {
+        const uint32_t x = (uint32_t)t, m = (uint32_t)g.mask;
+        const bool flip = g.n_ext > g.G;
+        uint32_t best = x;
+        int be = 0;
+        for (int gi = 0; gi < g.G; ++gi) {
+            const uint32_t y = apply_site_map32(g, sm, gi, x);
+            if (y < best) { best = y; be = gi; }
+            if (flip) {
+                const uint32_t yz = y ^ m;
+                if (yz < best) { best = yz; be = gi + g.G; }
+            }
+        }
+        if (be == 0 && best == x && apply_site_map32(g, sm, 0, x) != x) {
+            for (int e = 1; e < g.n_ext; ++e)
+                if (apply_elem(g, sm, e, t) == t) { be = e; break; }
+        }
+        *elem = be;
+        return best;
+    }
     uint64_t best = t;
     int be = 0;
     bool flip = g.n_ext > g.G;

@@ -107,8 +107,11 @@ __device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, 
     if (g.structured && g.L <= 32) {
         const uint32_t x = (uint32_t)s, m = (uint32_t)g.mask;
         const bool flip = g.n_ext > g.G;
+        // one row (a chain): every element is a rotation, read off the doubled word
+        const bool chain = g.W == g.L;
+        const uint64_t xx = ((uint64_t)x << g.L) | x;
         for (int gi = 0; gi < g.G; ++gi) {
-            const uint32_t y = apply_site_map32(g, sm, gi, x);
+            const uint32_t y = chain ? (uint32_t)(xx >> (g.L - (int)sm.rot[gi].ri)) & m : apply_site_map32(g, sm, gi, x);
             if (y < x) return false;
             if (flip && (y ^ m) < x) return false;
         }
@@ -130,8 +133,11 @@ __device__ __forceinline__ uint64_t orbit_min(const GroupArgs& g, const GroupSme
         const bool flip = g.n_ext > g.G;
         uint32_t best = x;
         int be = 0;
+        // one row (a chain): every element is a rotation, read off the doubled word
+        const bool chain = g.W == g.L;
+        const uint64_t xx = ((uint64_t)x << g.L) | x;
         for (int gi = 0; gi < g.G; ++gi) {
-            const uint32_t y = apply_site_map32(g, sm, gi, x);
+            const uint32_t y = chain ? (uint32_t)(xx >> (g.L - (int)sm.rot[gi].ri)) & m : apply_site_map32(g, sm, gi, x);
             if (y < best) { best = y; be = gi; }
             if (flip) {
                 const uint32_t yz = y ^ m;

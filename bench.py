@@ -616,6 +616,9 @@ def main():
                     help="time only the batched H*v kernels (small device footprint, for profiling)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison solve and the end-to-end repeat")
+    ap.add_argument("--profile-matrix-free", action="store_true",
+                    help="two matrix-free FP32 products on the L=32 J1-J2 k=0 even sector, then exit "
+                         "(the launch the matrix-free ncu summary profiles)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -645,6 +648,22 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import qmbcuda_b200 as q
+
+    if args.profile_matrix_free:
+        A = q._capi
+        L = 32
+        perm, ch = q.translation_group(L)
+        s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+        J = [1.0] * L + [0.5] * L
+        h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J), prec=A.PREC_FP32)
+        x = torch.randn(int(h.info.n_rows), dtype=torch.float32, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(2):
+            q.check(q.lib().qmb_hv_matrix_free(h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()),
+                                               A.C.c_void_p(y.data_ptr()), None))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "matrix-free FP32 product, L=32 J1-J2 k=0 even", "rows": int(h.info.n_rows)}))
+        return 0
 
     if args.hv_only:
         secs, b = build_batched(q)

@@ -472,19 +472,28 @@ def run_batched(args, torch, q, rank, world):
         e2e_t.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_t))
     # the same with the sectors and the batch built from scratch every step
-    setup_t = []
+    # (the batch above is released first, as a caller that rebuilds does:
+    # otherwise its Krylov ring holds the memory the new batch sizes its own
+    # ring from)
+    info = b.info
+    b.close()
+    setup_t, build_t = [], []
     for _ in range(0 if args.no_compare else max(1, min(3, args.steps))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s2, b2 = build_batched(q, L, n_sets)
+        tb = time.perf_counter()
         E2, r2 = b2.solve(J, J * D, **opts)
         t1 = time.perf_counter()
         setup_t.append(t1 - t0)
+        build_t.append(tb - t0)
         b2.close()
         for s in s2:
             s.close()
     e2e_setup = {"value": float(np.mean(hv_count)) / float(np.mean(setup_t)), "unit": "Hv/s",
-                 "s_per_step": float(np.mean(setup_t))} if setup_t else None
+                 "s_per_step": float(np.mean(setup_t)),
+                 "s_steps": [round(v, 4) for v in setup_t],
+                 "s_build_sectors_and_batch": [round(v, 4) for v in build_t]} if setup_t else None
     single = None if args.no_compare else single_sector_hv(torch, q)
     obs = None if args.no_compare else observables(torch, q)
     files = None if args.no_compare else table_files(torch, q)
@@ -507,9 +516,9 @@ def run_batched(args, torch, q, rank, world):
         "hv_kernel_gbs_fp64": info.bytes_hv_fp64 / (hv64_ms * 1e-3) / 1e9,
         "hv_ratio_fp32_over_fp64": hv64_ms / hv32_ms,
         "max_rel_dE0_mixed_vs_fp64": float(rel.max()),
-        "hv_tuner": {"variant_fp32": int(b.info.variant_fp32), "variant_fp64": int(b.info.variant_fp64),
-                     "ms_fp32": [round(v, 4) for v in b.info.tune_ms_fp32],
-                     "ms_fp64": [round(v, 4) for v in b.info.tune_ms_fp64],
+        "hv_tuner": {"variant_fp32": int(info.variant_fp32), "variant_fp64": int(info.variant_fp64),
+                     "ms_fp32": [round(v, 4) for v in info.tune_ms_fp32],
+                     "ms_fp64": [round(v, 4) for v in info.tune_ms_fp64],
                      "variants": "(unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4)"},
         "e2e_with_setup": e2e_setup,
         "single_sector_hv": single,

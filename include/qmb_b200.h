@@ -446,6 +446,9 @@ typedef struct {
     int variant_fp64;
     float tune_ms_fp32[4];  /* tuner timings of the variants, ms */
     float tune_ms_fp64[4];
+    int ring_slots[2];      /* FP32 Krylov vectors the handle's ring holds now, real and
+                               complex sectors (0: none yet); the ring starts at 128
+                               (QMB_RING_START) and doubles when a solve needs more */
 } qmb_batch_info;
 
 QMB_API qmb_status qmb_batch_create(const qmb_batch_desc* desc, qmb_batch* out);

@@ -16,11 +16,16 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+
+#include <cub/cub.cuh>
 
 #include "qmb_ham.cuh"
 #include "qmb_lanczos.cuh"
@@ -837,16 +842,26 @@ __global__ void k_britz(BLz lz, const int* __restrict__ msteps, const double* __
         const double sc = fmax(fabs(th), 1e-300);
         for (int i = 0; i < m; ++i) ritz[(int64_t)i * np + p] = 0.0;
         add_ritz_vector(lz, p, m, th, L, D, x, ritz);
+        // Ritz values 1..4, each found by bisection at most once
+        double tks[5];
+        int known = 1;
+        auto kth_value = [&](int kth) {
+            while (known <= kth) {
+                tks[known] = bis_kth(lz.alpha, lz.beta, np, p, m, known);
+                ++known;
+            }
+            return tks[kth];
+        };
         if (gap_out) {  // gap to the next Ritz value that is not a ghost copy
             double g = 1e-10 * sc;
             for (int kth = 1; kth < min(m, 5); ++kth) {
-                double tk = bis_kth(lz.alpha, lz.beta, np, p, m, kth);
+                double tk = kth_value(kth);
                 if (tk - th > 1e-10 * sc) { g = tk - th; break; }
             }
             gap_out[p] = g;
         }
         for (int kth = 1; kth < min(m, 4); ++kth) {
-            const double tk = bis_kth(lz.alpha, lz.beta, np, p, m, kth);
+            const double tk = kth_value(kth);
             if (tk - th > 1e-4 * sc) break;
             if (tk - th > 1e-10 * sc) add_ritz_vector(lz, p, m, tk, L, D, x, ritz);
         }
@@ -936,6 +951,94 @@ __global__ void k_bpsi(BatchArgs a, int64_t tot, const V* __restrict__ vring, in
     }
 }
 
+// ------------------------------------------------- batch assembly (device)
+// A SELL slice holds 32 rows; padding entries repeat the row index with a
+// zero value and are dropped (a zero entry contributes nothing).
+__device__ __forceinline__ bool sell_pad(uint32_t c, int64_t r, double v) { return c == (uint32_t)r && v == 0.0; }
+__device__ __forceinline__ bool sell_pad(uint32_t c, int64_t r, double2 v) {
+    return c == (uint32_t)r && v.x == 0.0 && v.y == 0.0;
+}
+__device__ __forceinline__ double2 widen2(double v) { return make_double2(v, 0.0); }
+__device__ __forceinline__ double2 widen2(double2 v) { return v; }
+
+// cnt[r] = entries of row r that are not padding (r < n); cnt[n] = 0.
+template <class VI>
+__global__ void k_sell_row_count(int64_t n, const int64_t* __restrict__ off, const int* __restrict__ w,
+                                 const uint32_t* __restrict__ col, const VI* __restrict__ val,
+                                 int64_t* __restrict__ cnt) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r <= n; r += (int64_t)gridDim.x * blockDim.x) {
+        if (r == n) { cnt[n] = 0; continue; }
+        const int64_t sl = r >> 5, lane = r & 31;
+        int64_t c = 0;
+        for (int jj = 0; jj < w[sl]; ++jj) {
+            const int64_t pos = off[sl] + (int64_t)jj * 32 + lane;
+            c += sell_pad(col[pos], r, val[pos]) ? 0 : 1;
+        }
+        cnt[r] = c;
+    }
+}
+
+// Row r's entries at rp[r].. in slice order (the order of the single-sector table).
+template <class VI>
+__global__ void k_sell_to_csr(int64_t n, const int64_t* __restrict__ off, const int* __restrict__ w,
+                              const uint32_t* __restrict__ col, const VI* __restrict__ val,
+                              const int64_t* __restrict__ rp, uint32_t* __restrict__ ocol,
+                              double2* __restrict__ oval) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t sl = r >> 5, lane = r & 31;
+        int64_t o = rp[r];
+        for (int jj = 0; jj < w[sl]; ++jj) {
+            const int64_t pos = off[sl] + (int64_t)jj * 32 + lane;
+            const uint32_t c = col[pos];
+            const VI v = val[pos];
+            if (sell_pad(c, r, v)) continue;
+            ocol[o] = c;
+            oval[o] = widen2(v);
+            ++o;
+        }
+    }
+}
+
+template <class VI>
+__global__ void k_widen(int64_t n, const VI* __restrict__ in, double2* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = widen2(in[i]);
+}
+
+__device__ __forceinline__ void narrow(double2 v, double& d, float& f) { d = v.x; f = (float)v.x; }
+__device__ __forceinline__ void narrow(double2 v, double2& d, float2& f) {
+    d = v;
+    f = make_float2((float)v.x, (float)v.y);
+}
+
+// One sector's CSR part and diagonals placed into its kind's arrays: row
+// pointers offset by the sector's first entry, values in FP64 and FP32.
+struct PlaceArgs {
+    int64_t n, nnz, ent0;
+    const int64_t* rp;
+    const uint32_t* col;
+    const double2 *val, *dxy, *dz;
+    int64_t* row_ptr;   // at the sector's row base
+    uint32_t* ocol;     // at the sector's first entry
+};
+template <class V64, class V32>
+__global__ void k_place_sector(PlaceArgs a, V64* __restrict__ val64, V32* __restrict__ val32,
+                               V64* __restrict__ dxy64, V32* __restrict__ dxy32, V64* __restrict__ dz64,
+                               V32* __restrict__ dz32) {
+    const int64_t m = a.n + 1 > a.nnz ? a.n + 1 : a.nnz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i <= a.n) a.row_ptr[i] = a.ent0 + a.rp[i];
+        if (i < a.nnz) {
+            a.ocol[i] = a.col[i];
+            narrow(a.val[i], val64[i], val32[i]);
+        }
+        if (i < a.n) {
+            narrow(a.dxy[i], dxy64[i], dxy32[i]);
+            narrow(a.dz[i], dz64[i], dz32[i]);
+        }
+    }
+}
+
 }  // namespace qmb
 
 using namespace qmb;
@@ -951,6 +1054,7 @@ struct BKind {
     DevBuf<unsigned> d_ctr;      // work queue head + retired blocks
     DevBuf<unsigned> d_sec_ctr;  // per-sector finished tiles
     int variant[2] = {-1, -1};    // tuned k_bhv variant per precision (FP32, FP64)
+    int ring_hint = 0;            // Krylov ring slots the phases on this handle needed
     DevBuf<unsigned char> ws_ring, ws_w;  // Lanczos workspace kept between solves
     std::unique_ptr<BKind> compact;        // descriptor of the last compacted sub-batch
     float tune_ms[2][4] = {};
@@ -1057,10 +1161,40 @@ static void bhv_variant(int variant, const BatchArgs& a, BKind& k, const V* x, V
 
 // Autotuner: times every variant on this batch's own matrices (plain H*v on
 // scratch vectors, best of 3) and keeps the fastest for the precision.
+// Tuner choices by batch shape (device, scalar size, padded sets, sectors,
+// tiles, largest tile, rows, entries), shared by the handles of a process.
+struct TuneKey {
+    int dev, vsize, nsp, n_sectors, n_tiles, max_tile;
+    int64_t rows, nnz;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(dev, vsize, nsp, n_sectors, n_tiles, max_tile, rows, nnz) <
+               std::tie(o.dev, o.vsize, o.nsp, o.n_sectors, o.n_tiles, o.max_tile, o.rows, o.nnz);
+    }
+};
+struct TuneEntry {
+    int variant = 0;
+    float ms[kBVariants] = {};
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneEntry> g_tune_cache;
+
 template <class V>
 static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st) {
     int& v = k.variant[f64 ? 1 : 0];
     if (v >= 0) return v;
+    // a batch of the same shape tuned before in this process reuses the choice
+    int dev = 0;
+    QMB_CUDA_TRY(cudaGetDevice(&dev));
+    const TuneKey key{dev, (int)sizeof(V), a.nsp, k.n_sectors, k.n_tiles, k.max_tile_entries, k.rows, k.nnz};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            for (int c = 0; c < kBVariants; ++c) k.tune_ms[f64 ? 1 : 0][c] = it->second.ms[c];
+            v = it->second.variant;
+            return v;
+        }
+    }
     const int64_t tot = k.sec_elem[k.n_sectors];
     DevBuf<V> x(tot), y(tot);
     QMB_CUDA_TRY(cudaMemsetAsync(x.p, 0, sizeof(V) * tot, st));
@@ -1098,6 +1232,13 @@ static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st
     cudaEventDestroy(e1);
     check_launch("k_bhv tuning");
     v = arg;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        if (g_tune_cache.size() >= 512) g_tune_cache.clear();
+        TuneEntry& e = g_tune_cache[key];
+        e.variant = arg;
+        for (int c = 0; c < kBVariants; ++c) e.ms[c] = tmin[c];
+    }
     return v;
 }
 
@@ -1126,6 +1267,15 @@ static void bnorm0_any(const BatchArgs& a, const BKind& k, const V* w, BLz lz, c
 
 // Krylov vectors of vec_bytes each that fit in about half of the free
 // device memory (at most want); 0 when fewer than 16 fit.
+constexpr int kRingStart = 128;  // first Krylov ring size of a handle, in vectors
+
+// QMB_RING_START=n (n >= 3) sets the first ring size instead (memory-tight runs).
+static int ring_start() {
+    const char* e = std::getenv("QMB_RING_START");
+    const int v = e ? std::atoi(e) : 0;
+    return v >= 3 ? v : kRingStart;
+}
+
 static int krylov_slots(size_t vec_bytes, int want, size_t cached = 0) {
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
@@ -1448,8 +1598,14 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     const int cap = std::max(1, max_iter);
     (void)minrows;
     // Krylov basis kept on the device (ring of K vectors); when the phase
-    // runs longer than the ring, the Ritz vector is regenerated instead
-    const int K = store_slots > 2 ? std::min(store_slots, cap + 1) : 2;
+    // runs longer than the ring, the Ritz vector is regenerated instead.
+    // K_full slots would hold the whole phase; the ring starts at what the
+    // earlier phases on this handle needed (at least kRingStart slots) and
+    // doubles when a phase reaches its end.
+    const size_t vec_bytes = std::max<size_t>((size_t)tot * sizeof(V), 1);
+    int K_full = store_slots > 2 ? std::min(store_slots, cap + 1) : 2;
+    int K = K_full > 2 ? std::min(K_full, std::max(ring_start(), k.ring_hint)) : 2;
+    if (K_full > 2) K = std::max(K, std::min(K_full, (int)(k.ws_ring.n / vec_bytes)));
     // workspace cached on the handle (grown on demand, reused by later solves)
     auto grow = [&](DevBuf<unsigned char>& buf, size_t bytes) {
         if (buf.n < bytes) {
@@ -1458,7 +1614,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
         }
     };
     grow(k.ws_w, 2 * (size_t)tot * sizeof(V));
-    grow(k.ws_ring, (size_t)K * tot * sizeof(V));
+    grow(k.ws_ring, (size_t)K * vec_bytes);
     struct View { V* p; } wbuf{reinterpret_cast<V*>(k.ws_w.p)}, vring{reinterpret_cast<V*>(k.ws_ring.p)};
     Buf<double> alpha = ws_take<double>((size_t)(cap + 1) * n_prob),
         beta = ws_take<double>((size_t)(cap + 2) * n_prob),
@@ -1515,12 +1671,37 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
         Buf<int> d_w = ws_take<int>(k.n_sectors);
         d_w.upload(wts.data(), k.n_sectors, st);
         const bool can_compact = !psi_out && K == 2;
-        LoopOut lo = device_loop(step, a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p,
-                                 theta_prev.p, msteps.p, conv.p, k.d_active.p, active_next.p, k.d_nrows.p, d_w.p,
-                                 k.n_sectors, std::max(1, check), 0, cap, can_compact ? 0.4 : 0.0, st);
+        LoopOut lo{0, 2, 0.0};
+        for (int j0 = 0;;) {
+            const int cap_run = K < K_full ? std::min(cap, K - 1) : cap;
+            lo = device_loop(step, a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p,
+                             theta_prev.p, msteps.p, conv.p, k.d_active.p, active_next.p, k.d_nrows.p, d_w.p,
+                             k.n_sectors, std::max(1, check), j0, cap_run, can_compact ? 0.4 : 0.0, st);
+            out.products += lo.products;
+            n_hv += lo.done - j0;
+            j0 = lo.done;
+            if (lo.reason != 2 || cap_run >= cap) break;
+            // the ring is full: continue in one twice as large, the filled
+            // slots copied over (slot i holds v_i while no slot was reused);
+            // without the memory the ring stays and wraps from here on
+            const int K2 = std::min(K_full, 2 * K);
+            void* np = nullptr;
+            if (cudaMalloc(&np, (size_t)K2 * vec_bytes) != cudaSuccess) {
+                (void)cudaGetLastError();
+                K_full = K;
+                continue;
+            }
+            QMB_CUDA_TRY(cudaMemcpyAsync(np, vring.p, (size_t)j0 * vec_bytes, cudaMemcpyDeviceToDevice, st));
+            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+            k.ws_ring.release();
+            k.ws_ring.p = reinterpret_cast<unsigned char*>(np);
+            k.ws_ring.n = (size_t)K2 * vec_bytes;
+            vring.p = reinterpret_cast<V*>(np);
+            K = K2;
+            if (trace_on()) std::fprintf(stderr, "[qmb batch] ring grown to %d slots at step %d\n", K, j0);
+        }
         done = lo.done;
-        out.products += lo.products;
-        n_hv += done;
+        if (K > 2) k.ring_hint = std::max(k.ring_hint, done + 1 + std::max(1, check));
         if (trace_on())
             std::fprintf(stderr, "[qmb batch] %s loop: %d steps, stop reason %d, %.2f ms to here\n",
                          f64 ? "fp64" : "fp32", done, lo.reason,
@@ -1622,15 +1803,24 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
         b->spl = spl_for<float2>(nsp);
         b->sector_kind.resize(d->n_sectors);
         b->sector_pos.resize(d->n_sectors);
-        // per-sector matrices through the single-sector builder
+        // per-sector matrices through the single-sector builder, turned into
+        // CSR on the device (the sector's SELL table never leaves HBM)
         struct Part {
-            std::vector<int64_t> row_ptr;
-            std::vector<uint32_t> col;
-            std::vector<double2> val;
-            std::vector<double2> dxy, dz;
+            std::vector<int64_t> row_ptr;      // host copy, for the tile tables
+            DevBuf<int64_t> rp;                // [n+1] entry offsets within the sector
+            DevBuf<uint32_t> col;              // [nnz]
+            DevBuf<double2> val, dxy, dz;      // [nnz], [n], [n]
         };
         std::vector<Part> parts(d->n_sectors);
+        const auto t_create = std::chrono::steady_clock::now();
+        double ms_build = 0.0, ms_csr = 0.0;
+        auto ms_since = [](std::chrono::steady_clock::time_point t) {
+            return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+        };
+        DevBuf<unsigned char> scan_tmp;
+        DevBuf<int64_t> row_cnt;
         for (int s = 0; s < d->n_sectors; ++s) {
+            auto t_part = std::chrono::steady_clock::now();
             qmb_sector sec = d->sectors[s];
             QMB_REQUIRE(sec && sec->has_irrep, QMB_ERR_INVALID, "every sector needs a selected irrep");
             QMB_REQUIRE(sec->device == d->device, QMB_ERR_INVALID, "sectors must live on the batch device");
@@ -1642,58 +1832,63 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             if (st != QMB_OK) throw Error{st, std::string("terms_z: ") + qmb_last_error()};
             std::unique_ptr<qmb_ham_s> oz(hz);
             QMB_REQUIRE(hz->nnz == 0, QMB_ERR_INVALID, "terms_z must be diagonal");
+            ms_build += ms_since(t_part);
+            t_part = std::chrono::steady_clock::now();
             const int64_t n = hx->n;
-            bool cplx = hx->cplx || hz->cplx;
-            b->sector_kind[s] = cplx ? 1 : 0;
-            // SELL -> CSR on the host (the shared tables are small)
-            std::vector<int64_t> off(hx->n_slices + 1);
-            std::vector<int> w(hx->n_slices);
-            hx->slice_off.download(off.data(), hx->n_slices + 1);
-            hx->slice_w.download(w.data(), hx->n_slices);
-            std::vector<uint32_t> col(std::max<int64_t>(hx->padded, 1));
-            std::vector<double2> val(std::max<int64_t>(hx->padded, 1));
-            std::vector<double2> dx(n), dz(n);
-            hx->col.download(col.data(), col.size());
-            if (hx->cplx) {
-                hx->val64.download(reinterpret_cast<unsigned char*>(val.data()), sizeof(double2) * val.size());
-                hx->diag64.download(reinterpret_cast<unsigned char*>(dx.data()), sizeof(double2) * n);
-            } else {
-                std::vector<double> tv(val.size()), td(n);
-                hx->val64.download(reinterpret_cast<unsigned char*>(tv.data()), sizeof(double) * tv.size());
-                hx->diag64.download(reinterpret_cast<unsigned char*>(td.data()), sizeof(double) * n);
-                for (size_t i = 0; i < tv.size(); ++i) val[i] = make_double2(tv[i], 0.0);
-                for (int64_t i = 0; i < n; ++i) dx[i] = make_double2(td[i], 0.0);
-            }
-            if (hz->cplx) {
-                hz->diag64.download(reinterpret_cast<unsigned char*>(dz.data()), sizeof(double2) * n);
-            } else {
-                std::vector<double> td(n);
-                hz->diag64.download(reinterpret_cast<unsigned char*>(td.data()), sizeof(double) * n);
-                for (int64_t i = 0; i < n; ++i) dz[i] = make_double2(td[i], 0.0);
-            }
-            QMB_CUDA_TRY(cudaDeviceSynchronize());
+            b->sector_kind[s] = (hx->cplx || hz->cplx) ? 1 : 0;
             Part& P = parts[s];
-            P.row_ptr.assign(1, 0);
-            for (int64_t r = 0; r < n; ++r) {
-                int64_t sl = r >> 5, lane = r & 31;
-                for (int jj = 0; jj < w[sl]; ++jj) {
-                    int64_t pos = off[sl] + (int64_t)jj * 32 + lane;
-                    double2 v = val[pos];
-                    if (col[pos] == (uint32_t)r && v.x == 0.0 && v.y == 0.0) continue;  // padding
-                    P.col.push_back(col[pos]);
-                    P.val.push_back(v);
-                }
-                P.row_ptr.push_back((int64_t)P.col.size());
+            P.rp.alloc(n + 1);
+            P.row_ptr.assign(n + 1, 0);
+            if (n == 0) P.rp.zero();
+            if (n > 0) {
+                const int gb = grid_for(n, 256);
+                if (row_cnt.n < (size_t)(n + 1)) row_cnt.alloc(n + 1);
+                if (hx->cplx)
+                    k_sell_row_count<double2><<<gb, 256>>>(n, hx->slice_off.p, hx->slice_w.p, hx->col.p,
+                                                           reinterpret_cast<const double2*>(hx->val64.p), row_cnt.p);
+                else
+                    k_sell_row_count<double><<<gb, 256>>>(n, hx->slice_off.p, hx->slice_w.p, hx->col.p,
+                                                          reinterpret_cast<const double*>(hx->val64.p), row_cnt.p);
+                check_launch("batch row counts");
+                size_t tb = 0;
+                QMB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, row_cnt.p, P.rp.p, n + 1));
+                if (scan_tmp.n < tb) scan_tmp.alloc(tb);
+                QMB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(scan_tmp.p, tb, row_cnt.p, P.rp.p, n + 1));
+                P.rp.download(P.row_ptr.data(), n + 1);
+                QMB_CUDA_TRY(cudaStreamSynchronize(0));
             }
-            P.dxy = std::move(dx);
-            P.dz = std::move(dz);
+            const int64_t nnz = P.row_ptr[n];
+            P.col.alloc(std::max<int64_t>(nnz, 1));
+            P.val.alloc(std::max<int64_t>(nnz, 1));
+            P.dxy.alloc(std::max<int64_t>(n, 1));
+            P.dz.alloc(std::max<int64_t>(n, 1));
+            if (n > 0) {
+                const int gb = grid_for(n, 256);
+                if (hx->cplx) {
+                    k_sell_to_csr<double2><<<gb, 256>>>(n, hx->slice_off.p, hx->slice_w.p, hx->col.p,
+                                                        reinterpret_cast<const double2*>(hx->val64.p), P.rp.p,
+                                                        P.col.p, P.val.p);
+                    k_widen<double2><<<gb, 256>>>(n, reinterpret_cast<const double2*>(hx->diag64.p), P.dxy.p);
+                } else {
+                    k_sell_to_csr<double><<<gb, 256>>>(n, hx->slice_off.p, hx->slice_w.p, hx->col.p,
+                                                       reinterpret_cast<const double*>(hx->val64.p), P.rp.p,
+                                                       P.col.p, P.val.p);
+                    k_widen<double><<<gb, 256>>>(n, reinterpret_cast<const double*>(hx->diag64.p), P.dxy.p);
+                }
+                if (hz->cplx) k_widen<double2><<<gb, 256>>>(n, reinterpret_cast<const double2*>(hz->diag64.p), P.dz.p);
+                else k_widen<double><<<gb, 256>>>(n, reinterpret_cast<const double*>(hz->diag64.p), P.dz.p);
+                check_launch("batch CSR");
+            }
+            // the builder's tables are freed with ox/oz: finish reading them first
+            QMB_CUDA_TRY(cudaStreamSynchronize(0));
+            ms_csr += ms_since(t_part);
         }
-        // assemble the two kinds
+        const auto t_assemble = std::chrono::steady_clock::now();
+        // assemble the two kinds: host tile tables, device placement of the parts
         for (int kd = 0; kd < 2; ++kd) {
             BKind& K = b->kind[kd];
-            std::vector<int64_t> row_ptr, row_base, row0;
-            std::vector<uint32_t> col;
-            std::vector<double2> val, dxy, dz;
+            std::vector<int64_t> row_base, row0, ent0;
+            int64_t n_rp = 0, n_ent = 0, n_rows = 0;
             K.sec_elem.assign(1, 0);
             for (int s = 0; s < d->n_sectors; ++s) {
                 if (b->sector_kind[s] != kd) continue;
@@ -1705,14 +1900,12 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                 K.nrows.push_back(n);
                 K.rows += n;
                 K.sec_elem.push_back(K.sec_elem.back() + n * b->nsp);
-                row_base.push_back((int64_t)row_ptr.size());
-                row0.push_back((int64_t)dxy.size());
-                int64_t eb = (int64_t)col.size();
-                for (int64_t r = 0; r <= n; ++r) row_ptr.push_back(eb + P.row_ptr[r]);
-                col.insert(col.end(), P.col.begin(), P.col.end());
-                val.insert(val.end(), P.val.begin(), P.val.end());
-                dxy.insert(dxy.end(), P.dxy.begin(), P.dxy.end());
-                dz.insert(dz.end(), P.dz.begin(), P.dz.end());
+                row_base.push_back(n_rp);
+                row0.push_back(n_rows);
+                ent0.push_back(n_ent);
+                n_rp += n + 1;
+                n_rows += n;
+                n_ent += P.row_ptr[n];
                 K.sec_tile0.push_back((int)K.tile_sector.size());
                 int nt = (int)((n + kBTile - 1) / kBTile);
                 K.sec_ntiles.push_back(nt);
@@ -1725,7 +1918,7 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
                 }
             }
             if (!K.n_sectors) continue;
-            K.nnz = (int64_t)col.size();
+            K.nnz = n_ent;
             K.n_tiles = (int)K.tile_sector.size();
             std::vector<int> tiles(K.n_tiles);
             for (int t = 0; t < K.n_tiles; ++t) tiles[t] = t;
@@ -1743,40 +1936,46 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             K.d_sec_ctr.zero();
             up_l(K.d_sec_elem, K.sec_elem);
             up_l(K.d_nrows, K.nrows);
-            up_l(K.d_row_ptr, row_ptr);
             up_l(K.d_row_base, row_base);
             up_l(K.d_row0, row0);
             K.h_row_base = row_base;
             K.h_row0 = row0;
-            K.d_col.alloc(std::max<size_t>(1, col.size()));
-            if (!col.empty()) K.d_col.upload(col.data(), col.size());
+            K.d_row_ptr.alloc(std::max<int64_t>(1, n_rp));
+            K.d_col.alloc(std::max<int64_t>(1, n_ent));
             // values in the sector kind's scalar types
-            auto store = [&](DevBuf<unsigned char>& d64, DevBuf<unsigned char>& d32, const std::vector<double2>& v) {
-                size_t n = std::max<size_t>(1, v.size());
-                if (kd == 1) {
-                    std::vector<float2> f(n);
-                    for (size_t i = 0; i < v.size(); ++i) f[i] = make_float2((float)v[i].x, (float)v[i].y);
-                    d64.alloc(n * sizeof(double2));
-                    d32.alloc(n * sizeof(float2));
-                    if (!v.empty()) d64.upload(reinterpret_cast<const unsigned char*>(v.data()), v.size() * sizeof(double2));
-                    d32.upload(reinterpret_cast<const unsigned char*>(f.data()), n * sizeof(float2));
-                } else {
-                    std::vector<double> r(n, 0.0);
-                    std::vector<float> f(n, 0.0f);
-                    for (size_t i = 0; i < v.size(); ++i) { r[i] = v[i].x; f[i] = (float)v[i].x; }
-                    d64.alloc(n * sizeof(double));
-                    d32.alloc(n * sizeof(float));
-                    d64.upload(reinterpret_cast<const unsigned char*>(r.data()), n * sizeof(double));
-                    d32.upload(reinterpret_cast<const unsigned char*>(f.data()), n * sizeof(float));
-                }
-            };
-            store(K.val64, K.val32, val);
-            store(K.dxy64, K.dxy32, dxy);
-            store(K.dz64, K.dz32, dz);
+            const size_t sv = kd ? sizeof(double2) : sizeof(double), sf = kd ? sizeof(float2) : sizeof(float);
+            K.val64.alloc(std::max<int64_t>(1, n_ent) * sv);
+            K.val32.alloc(std::max<int64_t>(1, n_ent) * sf);
+            K.dxy64.alloc(std::max<int64_t>(1, n_rows) * sv);
+            K.dxy32.alloc(std::max<int64_t>(1, n_rows) * sf);
+            K.dz64.alloc(std::max<int64_t>(1, n_rows) * sv);
+            K.dz32.alloc(std::max<int64_t>(1, n_rows) * sf);
+            for (int ks = 0; ks < K.n_sectors; ++ks) {
+                Part& P = parts[K.sec_index[ks]];
+                const int64_t n = K.nrows[ks], ne = P.row_ptr[n];
+                const int gb = grid_for(std::max<int64_t>(n + 1, ne), 256);
+                PlaceArgs pa{n, ne, ent0[ks], P.rp.p, P.col.p, P.val.p, P.dxy.p, P.dz.p,
+                             K.d_row_ptr.p + row_base[ks], K.d_col.p + ent0[ks]};
+                if (kd)
+                    k_place_sector<double2, float2><<<gb, 256>>>(
+                        pa, reinterpret_cast<double2*>(K.val64.p) + ent0[ks], reinterpret_cast<float2*>(K.val32.p) + ent0[ks],
+                        reinterpret_cast<double2*>(K.dxy64.p) + row0[ks], reinterpret_cast<float2*>(K.dxy32.p) + row0[ks],
+                        reinterpret_cast<double2*>(K.dz64.p) + row0[ks], reinterpret_cast<float2*>(K.dz32.p) + row0[ks]);
+                else
+                    k_place_sector<double, float><<<gb, 256>>>(
+                        pa, reinterpret_cast<double*>(K.val64.p) + ent0[ks], reinterpret_cast<float*>(K.val32.p) + ent0[ks],
+                        reinterpret_cast<double*>(K.dxy64.p) + row0[ks], reinterpret_cast<float*>(K.dxy32.p) + row0[ks],
+                        reinterpret_cast<double*>(K.dz64.p) + row0[ks], reinterpret_cast<float*>(K.dz32.p) + row0[ks]);
+                check_launch("batch placement");
+            }
         }
         b->cxy.alloc(b->nsp);
         b->cz.alloc(b->nsp);
         QMB_CUDA_TRY(cudaDeviceSynchronize());
+        if (trace_on())
+            std::fprintf(stderr, "[qmb batch] create: sector matrices %.1f ms, device CSR %.1f ms, "
+                         "assembly %.1f ms, total %.1f ms\n", ms_build, ms_csr,
+                         ms_since(t_assemble), ms_since(t_create));
         *out = b.release();
     });
 }
@@ -1816,6 +2015,11 @@ extern "C" qmb_status qmb_batch_get_info(qmb_batch b, qmb_batch_info* info) {
         for (int c = 0; c < 4; ++c) {
             info->tune_ms_fp32[c] = kc.tune_ms[0][c];
             info->tune_ms_fp64[c] = kc.tune_ms[1][c];
+        }
+        for (int kd = 0; kd < 2; ++kd) {
+            const BKind& k = b->kind[kd];
+            const size_t vb = (size_t)k.sec_elem.back() * (kd ? sizeof(float2) : sizeof(float));
+            info->ring_slots[kd] = (k.n_sectors && vb) ? (int)(k.ws_ring.n / vb) : 0;
         }
     });
 }

@@ -113,3 +113,33 @@ def test_batch_many_sets_dense_oracle(mode):
         e = np.linalg.eigvalsh(H)[:, 0]
         err = np.abs(E[:, a] - e) / np.maximum(np.abs(e), 1.0)
         assert err.max() <= tol, (a, err.max(), int(err.argmax()))
+
+
+def test_batch_ring_growth_bit_identical(monkeypatch):
+    """A Krylov ring that starts at 4 vectors doubles until the FP32 phase
+    fits: the solve is bit-identical to one whose ring held the phase from
+    the start, and the ring ends no larger than its growth needed."""
+    L, n_sets = 10, 40
+    bonds = q.chain_bonds(L)
+    rng = np.random.default_rng(11)
+    D = rng.uniform(0, 2, n_sets)
+    J = rng.uniform(0.5, 1.5, n_sets)
+    out = []
+    for start in (None, "4"):
+        if start is None:
+            monkeypatch.delenv("QMB_RING_START", raising=False)
+        else:
+            monkeypatch.setenv("QMB_RING_START", start)
+        secs, perm, ch = _sectors(L)
+        b = q.Batch(secs, q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"),
+                    n_sets)
+        E, r = b.solve(J, J * D, mode=A.MODE_MIXED, max_iter=300, tol=1e-12)
+        out.append((E, r.iters, r.iters_low, list(b.info.ring_slots)))
+        b.close()
+    (E0, it0, lo0, ring0), (E1, it1, lo1, ring1) = out
+    assert np.array_equal(E0.view(np.uint64), E1.view(np.uint64))
+    assert (it0, lo0) == (it1, lo1)
+    assert min(ring0) >= 128
+    # grown from 4 by doubling; the longer FP32 phase (iters_low steps) fits
+    assert all(s in (4, 8, 16, 32, 64, 128, 256) for s in ring1), ring1
+    assert max(ring1) >= lo1 + 1 and max(ring1) <= 2 * (lo1 + 10), (ring1, lo1)

@@ -82,6 +82,9 @@ class Clocks:
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
+            # let nvidia-smi finish starting up (its NVML initialisation)
+            # before the first timed step; sampling runs throughout
+            time.sleep(0.5)
         except OSError:
             self.p = None
         return self

@@ -538,7 +538,7 @@ def run_batched(args, torch, q, rank, world):
                 e2e_value=float(np.mean(hv_count)) / e2e_s,
                 h2d=2 * n_sets * 8, d2h=n_sets * L * 8, roof_bytes=roof_bytes, roof_ms=hv32_ms,
                 launches=launches,
-                kernel="k_bhv (batched H*v, FP32; one launch for the complex sectors, one for the real ones)",
+                kernel="k_bhv (batched H*v, FP32, one launch per sector kind; the real momenta k=0, 10 are solved in the complex kind)",
                 dtype="f32+f64")
 
 

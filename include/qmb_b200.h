@@ -462,8 +462,11 @@ QMB_API qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const double
  * qmb_batch_layout (FP64: double / complex double; FP32: float / complex
  * float).  prec: QMB_PREC_FP64 or QMB_PREC_FP32. */
 QMB_API qmb_status qmb_batch_hv(qmb_batch b, int prec, const void* x_dev, void* y_dev, void* stream);
-/* Device vector layout: real sectors first, then complex sectors; each
- * sector is [row][set] with set stride info.set_stride.  offsets[s] is the
+/* Device vector layout: sectors of the real kind first, then those of the
+ * complex kind (is_complex[s] tells which; real sectors that have fewer than
+ * a quarter of the complex sectors' rows are stored and solved complex, with
+ * zero imaginary parts); each sector is [row][set] with set stride
+ * info.set_stride.  offsets[s] is the
  * start of caller sector s in scalars (a complex element counts 2);
  * offsets[n_sectors] is the total. */
 QMB_API qmb_status qmb_batch_layout(qmb_batch b, int64_t* offsets /* [n_sectors+1] */,

@@ -112,6 +112,7 @@ struct BLz {
     unsigned* sec_ctr;       // [n_sectors] tiles finished in the current kernel
     const int* sec_tile0;    // [n_sectors]
     const int* sec_ntiles;   // [n_sectors]
+    double gap_cap = kRestartGapCap;  // restart gap cap relative to |theta| (with a phase-1 gap)
 };
 
 // Called by every thread of a block after it wrote the partials of one tile
@@ -716,7 +717,8 @@ __global__ void k_bcheck(BatchArgs a, BLz lz, int nsets, double stall, double re
                     const double tk = warp_kth_eig(sa, sb2, me, cg, xg, ghi, 0.0, 1e-7 * (ghi - th));
                     if (tk - th > 1e-10 * sc) own_gap = tk - th;
                 }
-                const double gap = gap_in ? fmax(gap_in[p], 1e-10 * sc) : own_gap;
+                const double gap = gap_in ? fmin(fmin(fmax(gap_in[p], 1e-10 * sc), lz.gap_cap * sc), own_gap)
+                                          : own_gap;
                 // energy bound plus a settled theta (a close level not yet
                 // resolved keeps theta moving while the gap estimate is too large)
                 if (e_tol > 0 && !first && est * est / gap <= e_tol * sc && fabs(th - prev) <= e_tol * sc)
@@ -1265,9 +1267,10 @@ static void bnorm0_any(const BatchArgs& a, const BKind& k, const V* w, BLz lz, c
     k_bnorm0<V><<<k.n_tiles, a.nsp, 0, st>>>(a, k.n_tiles, w, lz);
 }
 
-// Krylov vectors of vec_bytes each that fit in about half of the free
-// device memory (at most want); 0 when fewer than 16 fit.
 constexpr int kRingStart = 128;  // first Krylov ring size of a handle, in vectors
+// real sectors with fewer rows than this fraction of the complex ones are
+// solved in the complex kind
+constexpr double kMergeRealFrac = 0.25;
 
 // QMB_RING_START=n (n >= 3) sets the first ring size instead (memory-tight runs).
 static int ring_start() {
@@ -1276,6 +1279,8 @@ static int ring_start() {
     return v >= 3 ? v : kRingStart;
 }
 
+// Krylov vectors of vec_bytes each that fit in about half of the free
+// device memory (at most want); 0 when fewer than 16 fit.
 static int krylov_slots(size_t vec_bytes, int want, size_t cached = 0) {
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
@@ -1537,6 +1542,7 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     iter.upload(&j, 1, st);
     check_launch("compaction");
     BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob_c, ck.d_sec_ctr.p, ck.d_sec_tile0.p, ck.d_sec_ntiles.p};
+    lz.gap_cap = restart_gap_cap();
     auto step = [&](cudaStream_t ss) {
         bhv_any<V>(ac, ck, wc.p, wc.p, vc.p, 2, lz, nullptr, nullptr, 1, ss);
         bupdate_any<V>(ac, ck, wc.p, vc.p, 2, lz, ss);
@@ -1646,6 +1652,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
     a.dz = f64 ? k.dz64.p : k.dz32.p;
     BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob, k.d_sec_ctr.p, k.d_sec_tile0.p, k.d_sec_ntiles.p};
+    lz.gap_cap = restart_gap_cap();
     const int rb = 256, rg = (n_prob + rb - 1) / rb;
     tuned_variant<V>(a, k, f64, st);
     g_kernels += 1;
@@ -1882,6 +1889,20 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
             // the builder's tables are freed with ox/oz: finish reading them first
             QMB_CUDA_TRY(cudaStreamSynchronize(0));
             ms_csr += ms_since(t_part);
+        }
+        // Real sectors that are a small part of a batch with complex ones join
+        // the complex kind (zero imaginary parts): on their own, their
+        // phases would be launch- and latency-bound steps run one after the
+        // other with the complex kind's.
+        {
+            int64_t rows_kind[2] = {0, 0};
+            for (int s = 0; s < d->n_sectors; ++s)
+                rows_kind[b->sector_kind[s]] += (int64_t)parts[s].row_ptr.size() - 1;
+            const char* me = std::getenv("QMB_MERGE_REAL");
+            const bool merge = !(me && me[0] == '0');
+            if (merge && rows_kind[0] > 0 && rows_kind[1] > 0 &&
+                (double)rows_kind[0] < kMergeRealFrac * (double)rows_kind[1])
+                for (int s = 0; s < d->n_sectors; ++s) b->sector_kind[s] = 1;
         }
         const auto t_assemble = std::chrono::steady_clock::now();
         // assemble the two kinds: host tile tables, device placement of the parts

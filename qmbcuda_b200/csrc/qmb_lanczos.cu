@@ -340,6 +340,7 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
                    DevBuf<V>& wbuf, LzState& st, cudaStream_t s) {
     const int64_t n = op.n;
     PhaseOut out;
+    const double gap_cap = restart_gap_cap();
     int cap = std::max(1, po.max_iter);
     K = store ? cap + 1 : 2;
     vring.alloc((size_t)K * n);
@@ -453,7 +454,9 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
             }
         }
         if (po.tol > 0 && done >= po.min_iter) {
-            const double gap = po.gap_in > 0 ? std::max(po.gap_in, 1e-10 * scale) : out.gap;
+            const double gap = po.gap_in > 0
+                                   ? std::min({std::max(po.gap_in, 1e-10 * scale), gap_cap * scale, out.gap})
+                                   : out.gap;
             // energy bound plus a settled theta (an unresolved close level
             // keeps theta moving while the gap estimate is too large)
             bool e_ok = po.e_tol > 0 && have_prev && est * est / gap <= po.e_tol * scale &&

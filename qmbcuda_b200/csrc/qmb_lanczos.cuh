@@ -1,8 +1,31 @@
 // qmb_lanczos.cuh -- device reductions shared by the Lanczos engines.
 #pragma once
+#include <cstdlib>
 #include "qmb_scalar.cuh"
 
 namespace qmb {
+
+// Gap cap of an FP64 restart from an FP32 Ritz vector, relative to |theta|.
+// Two levels closer than the FP32 phase resolves (about 1e-6 |theta|) look
+// like one Ritz value there, so the FP32 gap to the next visible level says
+// nothing about them: the restart's Ritz vector can be a blend c1 u1 + c2 u2
+// of the pair, with a residual of |c1 c2| times their splitting and an
+// energy between the two.  The restart bounds its energy error with a gap of
+// at most cap |theta|, so it accepts only residuals below sqrt(tol cap) |theta|
+// and keeps going until such a pair separates, unless the FP32 vector holds
+// almost none of the lower level (|c1 / c2| below about that bound over the
+// splitting).  On an L=20 pair split by 1.2e-7 |theta|, 256 start vectors:
+// 8 end on the upper level at cap 1e-4, 32 at 1e-3, 1 at 1e-5, none at 1e-6,
+// against 126 without a cap; the L=20 batch solve takes 119, 111, 131 and
+// 105 ms at caps 1e-4, 1e-3, 1e-5 and none.
+constexpr double kRestartGapCap = 1e-4;
+
+// The cap in effect: QMB_RESTART_GAP_CAP=x (x > 0) replaces the default.
+inline double restart_gap_cap() {
+    const char* e = std::getenv("QMB_RESTART_GAP_CAP");
+    const double v = e ? std::atof(e) : 0.0;
+    return v > 0.0 ? v : kRestartGapCap;
+}
 
 // Sum over the block; valid in thread 0.  Fixed shuffle tree, so the result
 // depends only on the per-thread inputs (deterministic).

@@ -143,3 +143,58 @@ def test_batch_ring_growth_bit_identical(monkeypatch):
     # grown from 4 by doubling; the longer FP32 phase (iters_low steps) fits
     assert all(s in (4, 8, 16, 32, 64, 128, 256) for s in ring1), ring1
     assert max(ring1) >= lo1 + 1 and max(ring1) <= 2 * (lo1 + 10), (ring1, lo1)
+
+
+def test_batch_real_sectors_alone_and_in_complex_kind():
+    """Real sectors form their own kind when the batch has no complex ones,
+    and join the complex kind when they are a small part of it (L=12: two
+    real momenta of twelve).  Both give the single-sector FP64 energies."""
+    L, n_sets = 12, 16
+    secs, perm, ch = _sectors(L)
+    bonds = q.chain_bonds(L)
+    txy, tz = q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z")
+    J = np.linspace(0.6, 1.4, n_sets)
+    D = np.linspace(0.1, 1.9, n_sets)
+    real = [secs[0], secs[L // 2]]
+    b_real = q.Batch(real, txy, tz, n_sets)
+    b_all = q.Batch(secs, txy, tz, n_sets)
+    assert list(b_real.layout()[1]) == [0, 0]
+    cp_all = b_all.layout()[1]
+    assert cp_all[0] == 1 and cp_all[L // 2] == 1 and all(cp_all)
+    for mode in (A.MODE_FP64, A.MODE_MIXED):
+        E_real, _ = b_real.solve(J, J * D, mode=mode, max_iter=300, tol=1e-12)
+        E_all, _ = b_all.solve(J, J * D, mode=mode, max_iter=300, tol=1e-12)
+        for i in (0, 9, n_sets - 1):
+            for col, a in ((0, 0), (1, L // 2)):
+                t = q.xxz_terms(bonds, J[i], J[i] * D[i])
+                e1 = q.Hamiltonian(secs[a], t).lanczos(tol=1e-12).E0
+                assert abs(E_real[i, col] - e1) <= 1e-10 * abs(e1), (mode, i, a)
+                assert abs(E_all[i, a] - e1) <= 1e-10 * abs(e1), (mode, i, a)
+
+
+def test_mixed_restart_near_degenerate_pair():
+    """L=20 XXZ chain at Delta = 7.2e-5, k = pi: the two lowest levels are
+    1.2e-7 |E| apart, below what the FP32 phase separates.  With 256 start
+    vectors (one per coupling set, all sets equal) the mixed solve must end
+    on the ground level for all but a few starts whose FP32 vector holds
+    almost none of it, and never further off than the splitting.  FP64 mode
+    has the same exposure, for starts that hold almost none of the ground
+    level (one of these 256)."""
+    L, n_sets = 20, 256
+    J0, D = 1.0086762452351132, 7.209233047955621e-05
+    perm, ch = q.translation_group(L)
+    bonds = q.chain_bonds(L)
+    s = q.Sector(L, L // 2, perm).set_irrep(ch[L // 2])
+    e_ref = q.Hamiltonian(s, q.xxz_terms(bonds, J0, J0 * D)).lanczos(
+        mode=A.MODE_FP64, tol=1e-14, max_iter=600, reorth=2).E0
+    b = q.Batch([s], q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"), n_sets)
+    J, JD = np.full(n_sets, J0), np.full(n_sets, J0 * D)
+    split = 1.2e-7
+    E64, _ = b.solve(J, JD, mode=A.MODE_FP64, max_iter=300, tol=1e-12)
+    err64 = np.abs(E64[:, 0] - e_ref) / abs(e_ref)
+    assert err64.max() <= split and (err64 > 1e-9).sum() <= 4, int((err64 > 1e-9).sum())
+    Em, _ = b.solve(J, JD, mode=A.MODE_MIXED, max_iter=300, tol=1e-12)
+    err = np.abs(Em[:, 0] - e_ref) / abs(e_ref)
+    assert err.max() <= split
+    # without the gap cap 126 of the 256 starts end on the upper level
+    assert (err > 1e-9).sum() <= 16, int((err > 1e-9).sum())

@@ -1184,6 +1184,16 @@ template <class V>
 static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st) {
     int& v = k.variant[f64 ? 1 : 0];
     if (v >= 0) return v;
+    // QMB_BHV_VARIANT=0..3 fixes the variant.  The variants may round the
+    // epilogue's products and sums differently (the compiler fuses them per
+    // instantiation), so fixing it makes results reproducible across machines.
+    if (const char* fe = std::getenv("QMB_BHV_VARIANT")) {
+        const int fv = std::atoi(fe);
+        if (fe[0] >= '0' && fe[0] <= '9' && fv >= 0 && fv < kBVariants) {
+            v = fv;
+            return v;
+        }
+    }
     // a batch of the same shape tuned before in this process reuses the choice
     int dev = 0;
     QMB_CUDA_TRY(cudaGetDevice(&dev));

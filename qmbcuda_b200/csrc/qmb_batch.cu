@@ -412,13 +412,15 @@ __global__ void k_brq_energy(int n_prob, const double* __restrict__ sums, double
 // r <= 1e-4 |E|; sectors with an unaccepted set stay active for the restart.
 __global__ void k_brq_accept(BatchArgs a, int n_prob, int nsets, const double* __restrict__ E,
                              const double* __restrict__ r2, const double* __restrict__ psi2,
-                             const double* __restrict__ gap, double tol, int* __restrict__ ok,
-                             int* __restrict__ active) {
+                             const double* __restrict__ gap, double tol, double gap_cap,
+                             int* __restrict__ ok, int* __restrict__ active) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_prob; p += gridDim.x * blockDim.x) {
         int s = p / a.nsp, set = p % a.nsp;
         double sc = fmax(fabs(E[p]), 1e-300);
         double r = sqrt(r2[p] / fmax(psi2[p], 1e-300));
-        double g = fmax(gap[p], 1e-10 * sc);
+        // the FP32 phase's gap, capped as in the restart (a pair of levels
+        // it did not separate would otherwise pass as converged)
+        double g = fmin(fmax(gap[p], 1e-10 * sc), gap_cap * sc);
         bool acc = r <= 1e-4 * sc && r * r / g <= tol * sc;
         ok[p] = acc ? 1 : 0;
         if (!acc && set < nsets) atomicOr(active + s, 1);
@@ -2233,7 +2235,8 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                         k_bsum<<<rg2, rb2, 0, st>>>(a, k.n_tiles, k.d_sec_tile0.p, k.d_sec_ntiles.p, part.p, 1, n_prob, r2.p);
                         act_d.zero(st);
                         g_kernels += 1;
-                        k_brq_accept<<<rg2, rb2, 0, st>>>(a, n_prob, b->n_sets, Eq.p, r2.p, sums.p + n_prob, gapb.p, tol64, ok.p, act_d.p);
+                        k_brq_accept<<<rg2, rb2, 0, st>>>(a, n_prob, b->n_sets, Eq.p, r2.p, sums.p + n_prob, gapb.p, tol64,
+                                                          restart_gap_cap(), ok.p, act_d.p);
                         check_launch("rq check");
                         Eq.download(e_rq.data(), n_prob, st);
                         act_d.download(act.data(), k.n_sectors, st);

@@ -119,6 +119,23 @@ def flush_l2(torch, buf):
 
 
 # --------------------------------------------------------------- workloads
+def batched_config(world: int, L: int = 20, n_sets: int = 256) -> dict:
+    """The batched workload's `config`, the same for both arms.  Every Sz=0
+    string lies in one orbit, and an orbit of d strings is active in d of the
+    L momentum sectors, so the sectors hold C(L, L/2) rows together."""
+    import math
+    rows = math.comb(L, L // 2)
+    return {
+        "workload": f"batched: {n_sets} XXZ chains L={L} periodic, Delta~U(0,2), J~U(0.5,1.5) "
+                    f"(mt19937-64 seed {SEED}), all k=0..{L - 1} of Sz=0, mixed precision",
+        "n_sets": n_sets, "L": L, "sectors": L, "problems": n_sets * L,
+        "rows_total": rows, "elements_per_hv": rows * n_sets,
+        "l2_policy": "x and y of one batched H*v (complex FP32, %.0f MB each) exceed L2; "
+                     "256 MB written between steps" % (rows * n_sets * 8 / 1e6),
+        "parallelism": f"dp{world} (independent coupling sets per GPU)",
+    }
+
+
 def build_batched(q, L=20, n_sets=256):
     perm, ch = q.translation_group(L)
     secs = [q.Sector(L, L // 2, perm).set_irrep(ch[a]) for a in range(L)]
@@ -500,15 +517,9 @@ def run_batched(args, torch, q, rank, world):
     single = None if args.no_compare else single_sector_hv(torch, q)
     obs = None if args.no_compare else observables(torch, q)
     files = None if args.no_compare else table_files(torch, q)
-    out = {
-        "workload": "batched: 256 XXZ chains L=20 periodic, Delta~U(0,2), J~U(0.5,1.5) "
-                    "(mt19937-64 seed 20261203), all k=0..19 of Sz=0, mixed precision",
-        "n_sets": n_sets, "L": L, "sectors": L, "problems": units,
-        "rows_total": int(info.rows_total), "elements_per_hv": int(info.elems_total),
-        "l2_policy": "vectors per batched H*v > L2 (FP32 %.0f MB); 256 MB written between steps"
-                     % (info.bytes_hv_fp32 / 1e6),
-        "parallelism": f"dp{world} (independent coupling sets per GPU)",
-    }
+    out = batched_config(world, L, n_sets)
+    # the batch's own counts (equal to the closed form above)
+    out["rows_total"], out["elements_per_hv"] = int(info.rows_total), int(info.elems_total)
     extra = {
         "sectors_per_s": units / (ms * 1e-3),
         "fp64_sectors_per_s": units / (r64.ms_total * 1e-3),
@@ -644,8 +655,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic", "impl": "reference",
-                "config": {"workload": "batched: 256 XXZ chains L=20, all k, reference CPU H*v sample",
-                           "parallelism": "host threads"},
+                "config": batched_config(args.gpus),
                 "cpu_baseline": {"value": v, "unit": "Hv/s", "cores": thr, "kind": "reference",
                                  "sample": sample},
                 "e2e": {"value": v, "unit": "Hv/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

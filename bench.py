@@ -69,10 +69,10 @@ class Clocks:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), f"qmb_bench_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(
@@ -554,12 +554,15 @@ def run_batched(args, torch, q, rank, world):
 
 
 def reference_tables(L=20, n_sets_sample=2):
-    """Reference-layout FP32 ELLs of the batched workload built by the
-    reference's own kernels (oracle/_ref, emulated on the host)."""
+    """Reference-layout FP32 ELLs of the batched workload (the first
+    `n_sets_sample` coupling sets x all L momenta), built by the reference's
+    own kernels (oracle/_ref, run on the host) from the oracle's group and
+    term tables.  Nothing here loads the product library.  Returns a list of
+    (ind, val, track, rows, W, k, set)."""
     import oracle as O
-    import qmbcuda_b200 as q
     R = O.ref()
-    perm, ch = q.translation_group(L)
+    g = O.translation_group(L)
+    perm = np.ascontiguousarray(g.perm, np.uint32)
     k = L // 2
     N = O.binom(L, k)
     G = L
@@ -567,51 +570,107 @@ def reference_tables(L=20, n_sets_sample=2):
     srs = np.zeros(N * G, np.uint32)
     norms = np.zeros(N * G, np.float32)
     oi = np.zeros(2 * N, np.uint32)
-    chf = np.ascontiguousarray(ch.astype(np.complex64)).view(np.float32).ravel()
-    Rn = R.ref_build_srs_complex(L, k, G, np.ascontiguousarray(perm), G, chf, reps, N, srs, norms, oi)
+    chf = np.ascontiguousarray(g.chars.astype(np.complex64)).view(np.float32).ravel()
+    Rn = R.ref_build_srs_complex(L, k, G, perm, G, chf, reps, N, srs, norms, oi)
     J, D = couplings(n_sets_sample)
     tabs = []
-    bonds = q.chain_bonds(L)
+    bonds = O.chain_bonds(L)
     W = 2 * L + 1
     for i in range(n_sets_sample):
-        t = q.xxz_terms(bonds, J[i], J[i] * D[i])
-        codes = np.ascontiguousarray(t.codes.ravel(), np.int32)
-        sites = np.ascontiguousarray(t.sites.ravel(), np.int32)
+        t = O.xxz_terms(bonds, J[i], J[i] * D[i])
+        codes = np.ascontiguousarray(t.codes, np.int32)
+        sites = np.ascontiguousarray(t.sites, np.int32)
+        n_ops = np.ascontiguousarray(t.n_ops, np.int32)
         sc = np.ascontiguousarray(t.scalar.astype(np.complex64)).view(np.float32).ravel()
         for a in range(L):
             ind = np.zeros(Rn * W, np.uint32)
             val = np.zeros(2 * Rn * W, np.float32)
             tr = np.zeros(Rn, np.int16)
-            R.ref_ham_terms_complex(L, k, G, Rn, srs, oi, G, chf, a, norms, 1e-5, t.n_terms, 2,
-                                    t.n_ops, codes, sites, sc, W, ind, val, tr)
-            tabs.append((ind, val, tr, Rn, W))
+            R.ref_ham_terms_complex(L, k, G, Rn, srs, oi, G, chf, a, norms, 1e-5, t.H, t.n_col,
+                                    n_ops, codes, sites, sc, W, ind, val, tr)
+            tabs.append((ind, val, tr, Rn, W, a, i))
     return tabs
 
 
+class ReferenceSweep:
+    """One "step" of the reference's CPU H*v on the batched workload: its
+    only CPU H*v, SparseMatDenseVec_prod_EEL_host (utils.cu:649-670, FP32),
+    once over every sampled sector matrix, row blocks on `threads` host
+    threads.  That function is float-only, so complex sectors (k != 0, L/2)
+    are timed on the real parts of their values: the same index and vector
+    traffic as the complex product, half of its arithmetic."""
+
+    def __init__(self, threads=None, L=20, n_sets_sample=2):
+        import ctypes as C
+        import oracle as O
+        self.R = O.ref()
+        self.threads = threads or os.cpu_count() or 1
+        tabs = reference_tables(L, n_sets_sample)
+        self.n = len(tabs)
+        self.rows = int(sum(t[3] for t in tabs))
+        self.desc = (f"{self.n} sector matrices ({n_sets_sample} coupling sets x {L} momenta) of the "
+                     f"L={L} batch, {self.rows} rows, one FP32 SparseMatDenseVec_prod_EEL_host per matrix "
+                     f"a step on {self.threads} threads; complex sectors on their real parts")
+        self._keep = []
+        ptrs = {k: [] for k in ("ind", "val", "tr", "x", "y")}
+        for j, (ind, val, tr, n, W, a, i) in enumerate(tabs):
+            vr = np.ascontiguousarray(val.reshape(-1, 2)[:, 0])
+            x = np.random.default_rng(j).standard_normal(n).astype(np.float32)
+            y = np.zeros(n, np.float32)
+            self._keep += [ind, vr, tr, x, y]
+            for key, arr in zip(("ind", "val", "tr", "x", "y"), (ind, vr, tr, x, y)):
+                ptrs[key].append(arr.ctypes.data)
+        self._arr = {key: (C.c_void_p * self.n)(*v) for key, v in ptrs.items()}
+        self.nobv = np.array([t[3] for t in tabs], np.int32)
+        self.W = np.array([t[4] for t in tabs], np.int32)
+
+    def step(self):
+        a = self._arr
+        self.R.ref_spmv_host_sweep(self.n, a["ind"], a["val"], a["tr"], a["x"], a["y"], self.nobv,
+                                   self.W, self.threads)
+
+    def run(self, steps, warmup):
+        """Seconds of each of `steps` timed steps after `warmup` untimed ones."""
+        for _ in range(warmup):
+            self.step()
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            self.step()
+            ts.append(time.perf_counter() - t0)
+        return ts
+
+
 def cpu_reference_hv(seconds=10.0, threads=None):
-    """The reference's CPU H*v (FP32 float path of SparseMatDenseVec_prod_EEL_host)
-    on the batched workload's sector matrices; complex sectors are timed on their
-    real part, which has the same index traffic (the reference's host H*v is
-    float-only).  Returns (Hv/s, threads, sample description)."""
-    import oracle as O
-    R = O.ref()
-    threads = threads or os.cpu_count() or 1
-    tabs = reference_tables()
-    xs = [np.random.default_rng(i).standard_normal(t[3]).astype(np.float32) for i, t in enumerate(tabs)]
-    reals = [np.ascontiguousarray(t[1].reshape(-1, 2)[:, 0]) for t in tabs]
-    ys = [np.zeros(t[3], np.float32) for t in tabs]
-    # warm
-    for (ind, val, tr, n, W), vr, x, y in zip(tabs, reals, xs, ys):
-        R.ref_spmv_host(ind, vr, tr, x, y, n, W, threads)
-    count = 0
-    t0 = time.perf_counter()
+    """The reference's CPU H*v (ReferenceSweep) repeated for about `seconds`.
+    Returns (Hv/s, threads, sample description)."""
+    sw = ReferenceSweep(threads)
+    sw.run(0, 1)
+    count, t0 = 0, time.perf_counter()
     while time.perf_counter() - t0 < seconds:
-        for (ind, val, tr, n, W), vr, x, y in zip(tabs, reals, xs, ys):
-            R.ref_spmv_host(ind, vr, tr, x, y, n, W, threads)
-            count += 1
+        sw.step()
+        count += sw.n
     dt = time.perf_counter() - t0
-    return count / dt, threads, f"{len(tabs)} sector matrices (2 coupling sets x 20 k) of L=20, " \
-                                f"{count} H*v in {dt:.1f} s"
+    return count / dt, sw.threads, f"{sw.desc}; {count} H*v in {dt:.1f} s"
+
+
+def reference_arm(args):
+    """bench.py --impl reference: the reference's own CPU H*v (ReferenceSweep)
+    on the batched workload, `args.warmup` untimed and `args.steps` timed
+    steps.  Returns the JSON line."""
+    sw = ReferenceSweep()
+    ts = sw.run(args.steps, args.warmup)
+    s = float(np.mean(ts))
+    v = sw.n / s
+    return {"metric": METRIC, "value": v, "unit": "Hv/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * s,
+            "ms_steps": [round(1e3 * t, 3) for t in ts],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": batched_config(args.gpus),
+            "cpu_baseline": {"value": v, "unit": "Hv/s", "cores": sw.threads, "kind": "reference",
+                             "sample": sw.desc},
+            "e2e": {"value": v, "unit": "Hv/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def aggregate_ranks(torch, dist, ms, e2e_s, units, device):
@@ -650,16 +709,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        v, thr, sample = cpu_reference_hv(args.cpu_seconds)
-        line = {"metric": METRIC, "value": v, "unit": "Hv/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic", "impl": "reference",
-                "config": batched_config(args.gpus),
-                "cpu_baseline": {"value": v, "unit": "Hv/s", "cores": thr, "kind": "reference",
-                                 "sample": sample},
-                "e2e": {"value": v, "unit": "Hv/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        print(json.dumps(reference_arm(args)))
         return 0
 
     import torch

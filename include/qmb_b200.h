@@ -47,7 +47,8 @@ typedef int qmb_status;
 #define QMB_ERR_NOMEM 3         /* device or host allocation failed               */
 #define QMB_ERR_ELL_OVERFLOW 4  /* a row needs more slots than the given width    */
 #define QMB_ERR_NOT_CONVERGED 5 /* Lanczos stopped at max_iter above tolerance    */
-#define QMB_ERR_TIMEOUT 6       /* a bounded device wait gave up                  */
+#define QMB_ERR_TIMEOUT 6       /* reserved: no entry point of this version spins on
+                                 * the device, so none returns it                 */
 #define QMB_ERR_UNSUPPORTED 7   /* valid request outside what this build handles  */
 #define QMB_ERR_NO_DEVICE 8     /* no CUDA device is visible                      */
 #define QMB_ERR_IO 9            /* a table file could not be opened, read or written */
@@ -341,9 +342,10 @@ QMB_API qmb_status qmb_lanczos_ref_ell(float* E, int n_iter, int nobv, int max_t
  * loaded.  Limits: nobv <= 262144 rows and n_iter <= 1024 steps; larger sizes
  * return QMB_ERR_INVALID (use qmb_lanczos_ref_ell for them).
  *
- * The first call on each device does the set-up (looks up the scratch
- * address, which loads the device code); make that first call before any
- * stream capture begins.  The scratch is shared by every call on a device in
+ * Every call looks up the scratch's device address on the current device
+ * (the first call on a device also loads the device code); make that first
+ * call before any stream capture begins.  The host-side work arrays (about
+ * 70 KB) are static too, not on the caller's stack.  The scratch is shared by every call on a device in
  * this process: calls that overlap on the GPU race on it.  This function
  * takes a process-wide lock and synchronises `stream` before it returns, so
  * host threads calling it are serialised. */

@@ -128,6 +128,9 @@ def ref():
                                     f32p, C.c_int, u32p, f32p, i16p]
         R.ref_spmv_host.restype = None
         R.ref_spmv_host.argtypes = [u32p, f32p, i16p, f32p, f32p, C.c_int, C.c_int, C.c_int]
+        R.ref_spmv_host_sweep.restype = None
+        R.ref_spmv_host_sweep.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, i32p, i32p, C.c_int]
         R.ref_spmv_kernel_complex.restype = None
         R.ref_spmv_kernel_complex.argtypes = [u32p, f32p, i16p, f32p, f32p, C.c_int, C.c_int]
         R.ref_init_random_vec.restype = None

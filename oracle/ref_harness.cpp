@@ -222,6 +222,34 @@ extern "C" void ref_spmv_host(const uint32_t* ind, const float* val, const short
     for (auto& t : pool) t.join();
 }
 
+/* One sweep of SparseMatDenseVec_prod_EEL_host (utils.cu:649-670) over
+ * n_mats matrices with a single pool of host threads: thread c takes the
+ * c-th contiguous row block of every matrix in turn, so thread start-up is
+ * paid once per sweep rather than once per matrix. */
+extern "C" void ref_spmv_host_sweep(int n_mats, const uint32_t* const* ind, const float* const* val,
+                                    const short* const* track, const float* const* x,
+                                    float* const* y, const int* nobv, const int* W,
+                                    int n_threads) {
+    if (n_threads < 1) n_threads = 1;
+    std::vector<std::thread> pool;
+    for (int c = 0; c < n_threads; ++c) {
+        pool.emplace_back([=] {
+            for (int m = 0; m < n_mats; ++m) {
+                int chunk = (nobv[m] + n_threads - 1) / n_threads;
+                int r0 = c * chunk;
+                int r1 = std::min(nobv[m], r0 + chunk);
+                if (r0 >= r1) continue;
+                SparseMatDenseVec_prod_EEL_host(
+                    const_cast<uint32_t*>(ind[m]) + (size_t)r0 * W[m],
+                    const_cast<float*>(val[m]) + (size_t)r0 * W[m],
+                    const_cast<short*>(track[m]) + r0, const_cast<float*>(x[m]), y[m] + r0,
+                    r1 - r0, W[m]);
+            }
+        });
+    }
+    for (auto& t : pool) t.join();
+}
+
 /* SparseMatDenseVec_prod_EEL<T> emulated (utils.cu:601-624; launch shape of
  * lanczos.cu:149-150,212-213). */
 extern "C" void ref_spmv_kernel_complex(const uint32_t* ind, const float* val, const short* track,

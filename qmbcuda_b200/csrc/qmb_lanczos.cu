@@ -869,24 +869,30 @@ static_assert(sizeof(double) * ((kNaMaxIter + 1) + (kNaMaxIter + 2) + kNaMaxIter
 
 static __device__ __align__(256) unsigned char g_na_scratch[kNaScratchBytes];
 
-constexpr int kNaMaxDevices = 64;
-std::mutex g_na_mutex;                          // one caller at a time per process
-unsigned char* g_na_ptr[kNaMaxDevices] = {};    // symbol address per device
+std::mutex g_na_mutex;  // one caller at a time per process
 
-// Once per device, with that device current: the address of the static
-// scratch.  The first call on a device loads this module's device code.
-unsigned char* na_scratch(int dev) {
-    QMB_REQUIRE(dev >= 0 && dev < kNaMaxDevices, QMB_ERR_UNSUPPORTED, "device ordinal beyond 63");
-    if (!g_na_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t ce = cudaGetSymbolAddress(&p, g_na_scratch);
-        if (ce != cudaSuccess || !p) {
-            cudaGetLastError();
-            throw Error{QMB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(ce)};
-        }
-        g_na_ptr[dev] = static_cast<unsigned char*>(p);
+// Host-side work arrays of a call (tridiagonal, Ritz coefficients and the
+// tridiagonal solver's workspace, about 70 KB), kept off the caller's stack
+// for callers on small-stack threads; g_na_mutex guards them.
+struct NaHost {
+    double ha[kNaMaxIter + 1], hb[kNaMaxIter + 2];
+    double sv[kNaMaxIter], work[4 * kNaMaxIter], cf[kNaMaxIter];
+    int iwork[kNaMaxIter];
+};
+NaHost g_na_host;
+
+// The device address of the static scratch on the current device, looked up
+// on every call (a device reset by the host application reloads the module,
+// which may move it).  The first call on a device loads this module's device
+// code.
+unsigned char* na_scratch() {
+    void* p = nullptr;
+    cudaError_t ce = cudaGetSymbolAddress(&p, g_na_scratch);
+    if (ce != cudaSuccess || !p) {
+        cudaGetLastError();
+        throw Error{QMB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(ce)};
     }
-    return g_na_ptr[dev];
+    return static_cast<unsigned char*>(p);
 }
 
 template <class V, class P>
@@ -921,13 +927,15 @@ void na_solve(unsigned char* base, const RefEllOp<V>& op, int n_iter, uint64_t s
         k_lz_update<V><<<nb, kLzBlock, 0, s>>>(n, wbuf, vring, K, d, 1);
     }
     check_launch("noalloc lanczos steps");
-    double ha[kNaMaxIter + 1], hb[kNaMaxIter + 2];
+    double* ha = g_na_host.ha;
+    double* hb = g_na_host.hb;
     QMB_CUDA_TRY(cudaMemcpyAsync(ha, d.alpha, sizeof(double) * n_iter, cudaMemcpyDeviceToHost, s));
     QMB_CUDA_TRY(cudaMemcpyAsync(hb, d.beta, sizeof(double) * (n_iter + 1), cudaMemcpyDeviceToHost, s));
     QMB_CUDA_TRY(cudaStreamSynchronize(s));
     int m = n_iter;
     for (int i = 0; i < n_iter; ++i) {
-        QMB_REQUIRE(std::isfinite(ha[i]), QMB_ERR_INVALID, "non-finite Lanczos coefficient (check the Hamiltonian)");
+        QMB_REQUIRE(std::isfinite(ha[i]) && std::isfinite(hb[i + 1]), QMB_ERR_INVALID,
+                    "non-finite Lanczos coefficient (check the Hamiltonian)");
         double sc_i = std::fabs(ha[i]) + (i > 0 ? std::fabs(hb[i]) : 0.0) + 1e-300;
         if (!(hb[i + 1] > 1e-13 * sc_i)) {  // invariant subspace reached
             m = i + 1;
@@ -935,9 +943,8 @@ void na_solve(unsigned char* base, const RefEllOp<V>& op, int n_iter, uint64_t s
         }
     }
     double theta = tridiag_min_eig(ha, hb + 1, m);
-    double sv[kNaMaxIter], work[4 * kNaMaxIter];
-    int iwork[kNaMaxIter];
-    tridiag_eigvec_ws(ha, hb + 1, m, theta, sv, work, iwork);
+    double* sv = g_na_host.sv;
+    tridiag_eigvec_ws(ha, hb + 1, m, theta, sv, g_na_host.work, g_na_host.iwork);
     for (int i = 0; i < n_iter; ++i) coeffs[i] = i < m ? sv[i] : 0.0;
     *E = theta;
     if (!res_ref) return;
@@ -975,12 +982,10 @@ extern "C" qmb_status qmb_lanczos_ref_ell_noalloc(float* E, int n_iter, int nobv
         QMB_REQUIRE(n_iter <= kNaMaxIter, QMB_ERR_INVALID,
                     "n_iter exceeds the 1024 steps of the static scratch (use qmb_lanczos_ref_ell)");
         std::lock_guard<std::mutex> lock(g_na_mutex);
-        int dev = 0;
-        QMB_CUDA_TRY(cudaGetDevice(&dev));
-        unsigned char* base = na_scratch(dev);
+        unsigned char* base = na_scratch();
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         double e0 = 0.0, rr = 0.0;
-        double cf[kNaMaxIter];
+        double* cf = g_na_host.cf;
         double* want_res = (residual && check_eig_state) ? &rr : nullptr;
         if (is_complex) {
             RefEllOp<float2> op{nobv, max_terms, ind_dev, (const float2*)val_dev, track_dev};

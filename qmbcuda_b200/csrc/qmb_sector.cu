@@ -13,6 +13,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "qmb_sector.cuh"
 
@@ -38,30 +40,42 @@ __device__ __forceinline__ uint64_t unrank(uint64_t r, int L, int k) {
     return s;
 }
 
-uint64_t host_binom(int n, int k) {
-    static uint64_t tab[65][65];
-    static bool ready = false;
-    if (!ready) {
+namespace {
+struct BinomTable {
+    uint64_t tab[65][65];
+    BinomTable() {
         for (int a = 0; a <= 64; ++a) {
             tab[a][0] = 1;
             for (int b = 1; b <= 64; ++b) tab[a][b] = a == 0 ? 0 : tab[a - 1][b - 1] + tab[a - 1][b];
         }
-        ready = true;
     }
+};
+}  // namespace
+
+uint64_t host_binom(int n, int k) {
+    static const BinomTable t;  // built once; thread-safe initialisation of a local static
     if (n < 0 || k < 0 || n > 64 || k > 64) return 0;
-    return tab[n][k];
+    return t.tab[n][k];
 }
 
+/* Copies the binomial table into this device's constant memory, once per
+ * device and process.  Several host threads may create sectors at once: the
+ * first one for a device uploads while the others wait on the same flag; an
+ * upload that throws leaves the flag unset, so the next call retries. */
 static void upload_binomials() {
     int dev = 0;
-    cudaGetDevice(&dev);
-    static bool done[64] = {false};
-    if (dev < 64 && done[dev]) return;
-    std::vector<uint64_t> t(65 * 65);
-    for (int n = 0; n <= 64; ++n)
-        for (int k = 0; k <= 64; ++k) t[n * 65 + k] = host_binom(n, k);
-    QMB_CUDA_TRY(cudaMemcpyToSymbol(c_binom, t.data(), sizeof(uint64_t) * t.size()));
-    if (dev < 64) done[dev] = true;
+    QMB_CUDA_TRY(cudaGetDevice(&dev));
+    static std::once_flag done[64];
+    auto upload = [] {
+        std::vector<uint64_t> t(65 * 65);
+        for (int n = 0; n <= 64; ++n)
+            for (int k = 0; k <= 64; ++k) t[n * 65 + k] = host_binom(n, k);
+        QMB_CUDA_TRY(cudaMemcpyToSymbol(c_binom, t.data(), sizeof(uint64_t) * t.size()));
+    };
+    if (dev >= 0 && dev < 64)
+        std::call_once(done[dev], upload);
+    else
+        upload();
 }
 
 // ------------------------------------------------------------------ kernels

@@ -77,3 +77,35 @@ def test_noalloc_rejects_sizes_beyond_the_scratch():
     st, *_ = _call(L.qmb_lanczos_ref_ell_noalloc, 1025, R, W, cplx, bufs, (None,))
     assert st == A.QMB_ERR_INVALID
     assert b"1024" in L.qmb_last_error()
+
+
+def test_noalloc_at_the_scratch_limit_complex_with_ritz_vector():
+    """nobv = 262144, the largest size the static scratch takes, with complex
+    values and the Ritz vector (check_eig_state = 1): the FP64 Ritz vector then
+    ends exactly at the end of the scratch's vector region.  The matrix is a
+    ring with random diagonal d_r and complex hopping t e^{i phi} between r and
+    r + 1 (reference ELL layout: slot 0 the diagonal, then r + 1 and r - 1)."""
+    import torch
+    n, W = 262144, 3
+    rng = np.random.default_rng(7)
+    d = rng.uniform(-1.0, 1.0, n)
+    hop = 0.8 * np.exp(1j * 0.3)
+    r = np.arange(n)
+    ind = np.stack([r, (r + 1) % n, (r - 1) % n], axis=1).astype(np.uint32)
+    val = np.stack([d.astype(np.complex128), np.full(n, hop), np.full(n, np.conj(hop))], axis=1)
+    tr = np.full(n, W, np.int16)
+    dind = torch.tensor(ind.astype(np.int64).ravel()).to(torch.int32).cuda()
+    dval = torch.tensor(np.ascontiguousarray(val.astype(np.complex64).ravel()).view(np.float32)).cuda()
+    dtr = torch.tensor(tr).cuda()
+    torch.cuda.synchronize()
+    bufs = (dind, dval, dtr)
+    n_iter = 60
+    L = q.lib()
+    st, e_ref, k_ref, r_ref = _call(L.qmb_lanczos_ref_ell, n_iter, n, W, True, bufs)
+    q.check(st)
+    for _ in range(2):
+        st, e, kr, res = _call(L.qmb_lanczos_ref_ell_noalloc, n_iter, n, W, True, bufs, (None,))
+        q.check(st)
+        assert abs(e - e_ref) <= 1e-6 * abs(e_ref), (e, e_ref)
+        assert np.max(np.abs(kr - k_ref)) <= 1e-5
+        assert abs(res - r_ref) <= 1e-5 * max(abs(r_ref), 1e-30) + 1e-12, (res, r_ref)

@@ -413,20 +413,84 @@ def single_sector_configs(torch, q):
     t0 = time.perf_counter()
     s = q.Sector(N * N, N * N // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
     t_sec = time.perf_counter() - t0
-    h = q.Hamiltonian(s, q.xxz_terms(q.square_bonds(N, N), 1.0, 1.0), prec=A.PREC_FP32)
+    h = q.Hamiltonian(s, q.xxz_terms(q.square_bonds(N, N), 1.0, 1.0), prec=A.PREC_FP32 | A.PREC_FP64)
     t_ham = time.perf_counter() - t0 - t_sec
     i = h.info
     ms32 = t_hv(h, A.PREC_FP32, False, 5)
+    ms64 = t_hv(h, A.PREC_FP64, False, 3)
     mf32 = t_hv(h, A.PREC_FP32, True, 2)
     gathers = float(i.nnz_offdiag) * 32.0  # one 32-byte DRAM sector per gathered x element
+
+    def once(**kw):
+        r = h.lanczos(allow_unconverged=True, **kw)
+        return {"ms": r.ms_total, "products": int(r.n_hv), "iters": [int(r.iters_low), int(r.iters)],
+                "E0": r.E0, "E0_per_site": r.E0 / (N * N), "residual": r.residual,
+                "converged": int(r.converged)}
+
+    # the configuration as stated: 200 FP32 steps (FP64 reductions), then the
+    # chosen mixed form (FP32 phase + FP64 restart) and a plain FP64 solve
+    fp32_200 = once(mode=A.MODE_FP32, max_iter=200, tol=0.0)
+    mixed = once(mode=A.MODE_MIXED, max_iter=200, tol=1e-12, refine_max_iter=200)
+    fp64 = once(mode=A.MODE_FP64, max_iter=300, tol=1e-12)
     out["6x6_k00_even"] = {
         "rows": int(i.n_rows), "nnz": int(i.nnz_offdiag), "sector_build_s": t_sec, "ham_build_s": t_ham,
         "hv_ms_fp32": ms32, "hv_gbs_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9,
         "hv_frac_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9 / peak,
         "hv_sector_gbs_fp32": gathers / (ms32 * 1e-3) / 1e9,
-        "hv_ms_matrix_free_fp32": mf32}
+        "hv_ms_fp64": ms64, "hv_gbs_fp64": i.bytes_fp64 / (ms64 * 1e-3) / 1e9,
+        "hv_ms_matrix_free_fp32": mf32,
+        "fp32_200_steps": fp32_200, "mixed": mixed, "fp64": fp64,
+        "rel_dE0_mixed_vs_fp64": abs(mixed["E0"] - fp64["E0"]) / abs(fp64["E0"]),
+        "rel_dE0_fp32_200_vs_fp64": abs(fp32_200["E0"] - fp64["E0"]) / abs(fp64["E0"]),
+        "E0_per_site_published": -0.678872,
+        "solve_speedup_mixed_over_fp64": fp64["ms"] / mixed["ms"]}
     h.close()
     s.close()
+    # the L=16 chain without symmetry: FP64, 150 steps, full reorthogonalisation
+    L = 16
+    s = q.Sector(L, L // 2, np.arange(L, dtype=np.uint32)[None]).set_irrep([1.0])
+    h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L), 1.0, 1.0))
+    h.lanczos(mode=A.MODE_FP64, max_iter=150, tol=0.0, reorth=2, seed=SEED)
+    r = h.lanczos(mode=A.MODE_FP64, max_iter=150, tol=0.0, reorth=2, seed=SEED)
+    out["L16_nosym_fp64_150"] = {"rows": int(h.info.n_rows), "ms": r.ms_total, "products": int(r.n_hv),
+                                 "E0": r.E0, "residual": r.residual}
+    h.close()
+    s.close()
+    return out
+
+
+def cpu_solve_baselines():
+    """The oracle's FP64 Lanczos (lanczos_fp64: scipy CSR products, full
+    reorthogonalisation through numpy/BLAS on all host threads) on the oracle's
+    own matrices of two single-sector configurations, timed on the host:
+      L=16 chain without symmetry (12,870 rows), 150 steps;
+      L=24 XXZ chain, Delta=0.5, k=0, spin-inversion even (56,450 rows), 120
+      steps (about twice what the GPU's FP64 solve needs).
+    The matrix build is not timed.  Returns {name: {s, steps, E0, ...}}."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    out = {}
+    cases = []
+    g = O.trivial_group(16)
+    sec = O.build_sector(g, 8)
+    t = O.xxz_terms(O.chain_bonds(16), 1.0, 1.0)
+    cases.append(("L16_nosym_fp64_150", sec, t, 0, 150))
+    g = O.translation_group(24, flip=True)
+    sec = O.build_sector(g, 12)
+    t = O.xxz_terms(O.chain_bonds(24), 1.0, 0.5)
+    cases.append(("L24_xxz_d0.5_k0_even", sec, t, 0, 120))
+    for name, sec, t, a, steps in cases:
+        rows = O.active_rows(sec, a)
+        rc, ind, val, tr = O.ell_terms(sec, t, a, 2 * t.H + 1)
+        M = O.ell_to_csr(ind, val, tr, rows).real.tocsr()
+        v0 = O.start_vector(SEED, M.shape[0])
+        t0 = time.perf_counter()
+        e0, al, be = O.lanczos_fp64(lambda v: M @ v, v0, steps, reorth=True)
+        dt = time.perf_counter() - t0
+        out[name] = {"rows": int(M.shape[0]), "steps": int(len(al)), "s": dt, "E0": e0,
+                     "cores": threads, "kind": "port",
+                     "sample": "oracle FP64 Lanczos with full reorthogonalisation (scipy CSR product on one "
+                               "thread, numpy/BLAS reorthogonalisation on all threads)"}
     return out
 
 
@@ -533,7 +597,8 @@ def run_batched(args, torch, q, rank, world):
         "hv_tuner": {"variant_fp32": int(info.variant_fp32), "variant_fp64": int(info.variant_fp64),
                      "ms_fp32": [round(v, 4) for v in info.tune_ms_fp32],
                      "ms_fp64": [round(v, 4) for v in info.tune_ms_fp64],
-                     "variants": "(unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4)"},
+                     "variants": "k_bhv (unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4); "
+                                 "k_bhv_s (streamed gathers) = (8,3) (6,4) (12,2) (16,2)"},
         "e2e_with_setup": e2e_setup,
         "single_sector_hv": single,
         "observables": obs,
@@ -771,6 +836,11 @@ def main():
         "clocks": res["clocks"], "gpu_launches": res["launches"],
     }
     line.update(res["extra"])
+    if rank == 0 and world == 1 and not args.no_compare:
+        try:
+            line["cpu_solve_baseline"] = cpu_solve_baselines()
+        except Exception as e:  # scipy or the oracle build absent
+            line["cpu_solve_baseline"] = {"unavailable": str(e)}
     if rank == 0 and world == 1:
         try:
             v, thr, sample = cpu_reference_hv(args.cpu_seconds)

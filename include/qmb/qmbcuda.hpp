@@ -32,9 +32,12 @@
  *    permutation array in the reference layout given directly.
  *  - The complex scalar is std::complex<float> unless the includer defines
  *    QMB_DROPIN_COMPLEX (e.g. as thrust::complex<float>) first.
- *  - The drivers solve each irrep to convergence (mixed FP32/FP64 Lanczos with
- *    an FP64 residual check) instead of a fixed NIter FP32 run, so E_vecs are
- *    the converged lowest energies; NIter and hop_f are accepted and unused.
+ *  - The drivers solve every irrep to convergence (mixed FP32/FP64 Lanczos
+ *    with an FP64 residual check) instead of a fixed NIter FP32 run, so E_vecs
+ *    are the converged lowest energies; NIter and hop_f are accepted and
+ *    unused.  Irreps holding at most 2^17 active rows together are solved in
+ *    one batched solve (qmb_batch_solve), larger ones one irrep at a time
+ *    (qmb_dropin::irrep_route() overrides the choice).
  *    LanczosEigVals_CUDA keeps the reference's fixed-NIter semantics.
  *  - Errors throw std::runtime_error with the library's message (the
  *    reference throws from its CHECK macros or exits).
@@ -269,6 +272,8 @@ public:
                                                op_site.data(), scalar.data(), &n));
         n_terms = n;
     }
+    LatticeGeometryInfo GetGeomInfo() { return geom_info; }
+    HeisenbergInfo<T> GetHeisenbergInfo() { return heisenberg_info; }
     qmb_terms terms() const {
         qmb_terms t;
         t.n_terms = n_terms;
@@ -312,6 +317,57 @@ inline SiteMap Cn(int n, std::vector<float> R0) {
             TR1[i] = (float)(std::cos(t) * x - std::sin(t) * y + R0[0]);
             TR2[i] = (float)(std::sin(t) * x + std::cos(t) * y + R0[1]);
         }
+    };
+}
+
+// Reflection across the line through the origin whose normal makes the
+// angle theta (degrees) with the x axis, as the reference's sigma_n_arb
+// (symmetries/SymmOperators.cu:21-36): r -> r - 2 n (n . r).
+inline SiteMap sigma_n_arb(float theta) {
+    return [theta](const std::vector<float>& R1, const std::vector<float>& R2, std::vector<float>& TR1,
+                   std::vector<float>& TR2) {
+        const double t = theta * 3.14159265358979323846 / 180.0;
+        const double nx = std::cos(t), ny = std::sin(t);
+        TR1.resize(R1.size());
+        TR2.resize(R2.size());
+        for (size_t i = 0; i < R1.size(); ++i) {
+            const double rp = nx * R1[i] + ny * R2[i];
+            TR1[i] = (float)(R1[i] - 2.0 * nx * rp);
+            TR2[i] = (float)(R2[i] - 2.0 * ny * rp);
+        }
+    };
+}
+
+// Shift by (nx, ny) on an Nx x Ny square lattice of unit spacing, wrapped by
+// fmod, as the reference's Tnm (symmetries/SymmOperators.cu:46-60).
+inline SiteMap Tnm(int Nx, int Ny, int nx, int ny) {
+    return [Nx, Ny, nx, ny](const std::vector<float>& R1, const std::vector<float>& R2, std::vector<float>& TR1,
+                            std::vector<float>& TR2) {
+        TR1.resize(R1.size());
+        TR2.resize(R2.size());
+        for (size_t i = 0; i < R1.size(); ++i) {
+            TR1[i] = std::fmod(R1[i] + (float)nx, (float)Nx);
+            TR2[i] = std::fmod(R2[i] + (float)ny, (float)Ny);
+        }
+    };
+}
+
+// Translation by nx a1 + ny a2 on the N1 x N2 torus of the geometry, as the
+// reference's Tnm_general (symmetries/SymmOperators.cu:62-126): the shifted
+// point's coefficients (c1, c2) in the basis (a1, a2) (from the Gram system
+// [[1, a1.a2], [a1.a2, 1]] c = (a1.r, a2.r), which takes |a1| = |a2| = 1 as
+// the reference does) are wrapped by fmod into [0, N1) x [0, N2); a
+// coefficient within 1e-3 of N counts as 0.
+inline SiteMap Tnm_general(int nx, int ny, LatticeGeometryInfo geom_info);
+
+// The composition G1(G2(r)), as the reference's GetElemProd
+// (symmetries/SymmOperators.cu:128-137).
+inline SiteMap GetElemProd(SiteMap G2, SiteMap G1) {
+    return [G2, G1](const std::vector<float>& R1, const std::vector<float>& R2, std::vector<float>& TR1,
+                    std::vector<float>& TR2) {
+        std::vector<float> a, b;
+        G2(R1, R2, a, b);
+        G1(a, b, TR1, TR2);
     };
 }
 
@@ -736,9 +792,58 @@ inline qmb_complex expval(GroundState& gs, const ManyBodyOperator<T>& A) {
     return make_scalar<qmb_complex>::from(out[0], out[1]);
 }
 
-// Lowest energy of every irrep of G for the given operator tables (one
-// sector handle, one Hamiltonian per irrep, mixed-precision Lanczos).  With
-// gs, the lowest state over all irreps is kept there.
+// Which route solve_irreps takes: 0 chooses by size (the batched solve when
+// all irreps together hold at most kBatchRows active rows, else one solve per
+// irrep), 1 always the batched solve, 2 always one solve per irrep.
+inline int& irrep_route() {
+    static int r = 0;
+    return r;
+}
+constexpr int64_t kBatchRows = 1 << 17;
+
+// Splits operator tables into the off-diagonal terms (any S+ or S- factor)
+// and the diagonal ones (Sz and identity factors only), the two parts a
+// batch takes; an empty part gets one term with a zero scalar.
+struct SplitTerms {
+    TermsCopy xy, z;
+    explicit SplitTerms(const qmb_terms& t) {
+        xy.n_col = z.n_col = t.n_col;
+        for (int i = 0; i < t.n_terms; ++i) {
+            bool diag = true;
+            for (int c = 0; c < t.n_ops[i]; ++c) {
+                const int code = t.op_code[(size_t)i * t.n_col + c];
+                if (code != QMB_OP_SZ && code != QMB_OP_I) diag = false;
+            }
+            TermsCopy& d = diag ? z : xy;
+            d.n_ops.push_back(t.n_ops[i]);
+            for (int c = 0; c < t.n_col; ++c) {
+                d.op_code.push_back(t.op_code[(size_t)i * t.n_col + c]);
+                d.op_site.push_back(t.op_site[(size_t)i * t.n_col + c]);
+            }
+            d.scalar.push_back(t.scalar[2 * i]);
+            d.scalar.push_back(t.scalar[2 * i + 1]);
+            ++d.n_terms;
+        }
+        for (TermsCopy* d : {&xy, &z})
+            if (d->n_terms == 0) {
+                d->n_terms = 1;
+                d->n_ops.assign(1, 1);
+                d->op_code.assign(t.n_col, QMB_OP_SZ);
+                d->op_site.assign(t.n_col, 0);
+                d->scalar.assign(2, 0.0);
+            }
+    }
+};
+
+// Lowest energy of every irrep of G for the given operator tables, with
+// mixed-precision Lanczos (FP32 phase, FP64 restart, FP64 residual).
+//  - Batched route: one sector handle per irrep and one qmb_batch_solve over
+//    all of them (one coupling set, the tables split into their off-diagonal
+//    and diagonal parts), the replacement of the reference driver's serial
+//    irrep loop (HeisenbergGenericXXZ_AbelianSymms_CUDA.cu:127-242).
+//  - Per-irrep route: one sector handle and one Hamiltonian per irrep.
+// With gs, the lowest state over all irreps is kept there (the batched route
+// solves that one irrep once more for its vector).
 template <class T>
 inline std::vector<std::vector<float>> solve_irreps(int L, int n_up, SymmetryClass<T>* G, const std::vector<float>& R1,
                                                     const std::vector<float>& R2, const qmb_terms& terms,
@@ -749,6 +854,7 @@ inline std::vector<std::vector<float>> solve_irreps(int L, int n_up, SymmetryCla
     std::vector<uint32_t> perm((size_t)nG * L);
     G->GetGroupElemArr(R1, R2, perm.data());
     std::vector<std::vector<T>> chars = G->GetCharTable();
+    const size_t n_irr = chars.size();
     qmb_sector_desc d;
     d.L = L;
     d.n_up = n_up;
@@ -756,50 +862,106 @@ inline std::vector<std::vector<float>> solve_irreps(int L, int n_up, SymmetryCla
     d.perm = perm.data();
     d.spin_flip = 0;
     d.device = 0;
-    qmb_sector s = nullptr;
-    check(qmb_sector_create(&d, &s));
-    std::vector<std::vector<float>> E(chars.size(), std::vector<float>(1, 1.0e7f));
-    try {
-        for (size_t a = 0; a < chars.size(); ++a) {
-            std::vector<double> c(2 * (size_t)nG);
-            for (int g = 0; g < nG; ++g) {
-                c[2 * g] = re(chars[a][g]);
-                c[2 * g + 1] = im(chars[a][g]);
+    std::vector<std::vector<double>> crow(n_irr, std::vector<double>(2 * (size_t)nG));
+    for (size_t a = 0; a < n_irr; ++a)
+        for (int g = 0; g < nG; ++g) {
+            crow[a][2 * g] = re(chars[a][g]);
+            crow[a][2 * g + 1] = im(chars[a][g]);
+        }
+    std::vector<std::vector<float>> E(n_irr, std::vector<float>(1, 1.0e7f));
+    // one sector per irrep with its irrep selected; irreps with no state are left out
+    std::vector<qmb_sector> secs(n_irr, nullptr);
+    auto release = [&] {
+        for (qmb_sector& x : secs)
+            if (x) qmb_sector_destroy(x), x = nullptr;
+    };
+    // the solve of one irrep (its Hamiltonian and Lanczos); with keep, its
+    // state replaces gs's when its energy is lower
+    auto solve_one = [&](size_t a, qmb_sector s, bool keep) -> double {
+        qmb_ham h = nullptr;
+        check(qmb_ham_create(s, &terms, QMB_PREC_FP64 | QMB_PREC_FP32, &h));
+        qmb_lanczos_opts o;
+        qmb_lanczos_default_opts(&o);
+        o.mode = QMB_MODE_MIXED;
+        o.seed = (uint64_t)seed;
+        o.want_vector = keep ? 1 : 0;
+        qmb_lanczos_result r;
+        qmb_status st = qmb_lanczos(h, &o, &r, nullptr, 0);
+        if (st == QMB_OK && keep && (float)r.E0 < gs->E) {
+            qmb_ham_info hi;
+            st = qmb_ham_get_info(h, &hi);
+            if (st == QMB_OK) {
+                gs->psi.assign((hi.is_complex ? 2 : 1) * (size_t)hi.n_rows, 0.0);
+                st = qmb_ground_state(h, gs->psi.data(), hi.n_rows);
+                gs->n_rows = hi.n_rows;
+                gs->E = (float)r.E0;
+                gs->irrep = (int)a;
+                gs->chars = crow[a];
             }
-            check(qmb_sector_set_irrep(s, c.data(), tol_norm));
+        }
+        qmb_ham_destroy(h);
+        check(st);
+        return r.E0;
+    };
+    try {
+        int64_t rows = 0;
+        std::vector<size_t> live;
+        for (size_t a = 0; a < n_irr; ++a) {
+            check(qmb_sector_create(&d, &secs[a]));
+            check(qmb_sector_set_irrep(secs[a], crow[a].data(), tol_norm));
             qmb_sector_info si;
-            check(qmb_sector_get_info(s, &si));
-            if (si.n_active == 0) continue;  // no state of this irrep
-            qmb_ham h = nullptr;
-            check(qmb_ham_create(s, &terms, QMB_PREC_FP64 | QMB_PREC_FP32, &h));
+            check(qmb_sector_get_info(secs[a], &si));
+            if (si.n_active == 0) {  // no state of this irrep
+                qmb_sector_destroy(secs[a]);
+                secs[a] = nullptr;
+                continue;
+            }
+            rows += si.n_active;
+            live.push_back(a);
+        }
+        const int route = irrep_route();
+        const bool batched = !live.empty() && (route == 1 || (route == 0 && rows <= kBatchRows));
+        if (batched) {
+            SplitTerms sp(terms);
+            const qmb_terms txy = sp.xy.view(), tz = sp.z.view();
+            std::vector<qmb_sector> ls;
+            for (size_t a : live) ls.push_back(secs[a]);
+            qmb_batch_desc bd;
+            bd.n_sectors = (int)ls.size();
+            bd.sectors = ls.data();
+            bd.terms_xy = &txy;
+            bd.terms_z = &tz;
+            bd.n_sets = 1;
+            bd.device = 0;
+            qmb_batch b = nullptr;
+            check(qmb_batch_create(&bd, &b));
             qmb_lanczos_opts o;
             qmb_lanczos_default_opts(&o);
             o.mode = QMB_MODE_MIXED;
             o.seed = (uint64_t)seed;
-            o.want_vector = gs ? 1 : 0;
+            const double one = 1.0;
+            std::vector<double> e0(ls.size());
             qmb_lanczos_result r;
-            qmb_status st = qmb_lanczos(h, &o, &r, nullptr, 0);
-            if (st == QMB_OK && gs && (float)r.E0 < gs->E) {
-                qmb_ham_info hi;
-                st = qmb_ham_get_info(h, &hi);
-                if (st == QMB_OK) {
-                    gs->psi.assign((hi.is_complex ? 2 : 1) * (size_t)hi.n_rows, 0.0);
-                    st = qmb_ground_state(h, gs->psi.data(), hi.n_rows);
-                    gs->n_rows = hi.n_rows;
-                    gs->E = (float)r.E0;
-                    gs->irrep = (int)a;
-                    gs->chars = c;
-                }
-            }
-            qmb_ham_destroy(h);
+            const qmb_status st = qmb_batch_solve(b, &one, &one, &o, e0.data(), &r);
+            qmb_batch_destroy(b);
             check(st);
-            E[a][0] = (float)r.E0;
+            size_t best = 0;
+            for (size_t i = 0; i < live.size(); ++i) {
+                E[live[i]][0] = (float)e0[i];
+                if (e0[i] < e0[best]) best = i;
+            }
+            if (gs) {
+                gs->E = 1.0e7f;
+                solve_one(live[best], secs[live[best]], true);
+            }
+        } else {
+            for (size_t a : live) E[a][0] = (float)solve_one(a, secs[a], gs != nullptr);
         }
     } catch (...) {
-        qmb_sector_destroy(s);
+        release();
         throw;
     }
-    qmb_sector_destroy(s);
+    release();
     if (gs) {
         gs->L = L;
         gs->n_up = n_up;

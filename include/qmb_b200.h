@@ -446,8 +446,8 @@ typedef struct {
     int set_stride;         /* sets per row in the device vector layout (padded) */
     int variant_fp32;       /* H*v kernel variant chosen by the tuner (-1: not tuned yet) */
     int variant_fp64;
-    float tune_ms_fp32[4];  /* tuner timings of the variants, ms */
-    float tune_ms_fp64[4];
+    float tune_ms_fp32[8];  /* tuner timings of the variants, ms */
+    float tune_ms_fp64[8];
     int ring_slots[2];      /* FP32 Krylov vectors the handle's ring holds now, real and
                                complex sectors (0: none yet); the ring starts at 128
                                (QMB_RING_START) and doubles when a solve needs more */

@@ -90,7 +90,7 @@ class BatchInfo(C.Structure):
                 ("bytes_hv_fp64", C.c_double), ("bytes_hv_fp32", C.c_double),
                 ("rows_per_block", C.c_int), ("sets_per_thread", C.c_int),
                 ("set_stride", C.c_int), ("variant_fp32", C.c_int), ("variant_fp64", C.c_int),
-                ("tune_ms_fp32", C.c_float * 4), ("tune_ms_fp64", C.c_float * 4),
+                ("tune_ms_fp32", C.c_float * 8), ("tune_ms_fp64", C.c_float * 8),
                 ("ring_slots", C.c_int * 2)]
 
 

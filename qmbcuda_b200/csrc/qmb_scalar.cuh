@@ -32,6 +32,9 @@ template <> struct Sc<float> {
     __host__ __device__ static float add(float a, float b) { return a + b; }
     __host__ __device__ static float sub(float a, float b) { return a - b; }
     __host__ __device__ static float scale(float a, double s) { return (float)(a * s); }
+    // a float factor: the product of two floats is exact in double, so the
+    // rounded float product equals the double form above
+    __host__ __device__ static float scale(float a, float s) { return a * s; }
     __host__ __device__ static float fma(float a, float b, float c) { return fmaf(a, b, c); }
     __host__ __device__ static double re_conj_mul(float a, float b) { return (double)a * b; }
     __host__ __device__ static double im_conj_mul(float, float) { return 0.0; }
@@ -87,6 +90,8 @@ template <> struct Sc<float2> {
     __host__ __device__ static float2 scale(float2 a, double s) {
         return make_float2((float)(a.x * s), (float)(a.y * s));
     }
+    // a float factor: same rounding as the double form (exact double product)
+    __host__ __device__ static float2 scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
     __host__ __device__ static float2 fma(float2 a, float2 b, float2 c) {
         return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
     }

@@ -15,6 +15,10 @@
 //  6. ComputeStaticExpValZeroT on the kept ground states of checks 1 and 4:
 //     <Sz0 Sz1> = E/(3L), <Sz0 Sz3>, <S+0 S-1> = 2 <Sz0 Sz1> and the structure
 //     factor at k = pi from FullFourierOperator, against dense FP64 values.
+//  7. The two routes of the drivers give the same energy in every irrep: the
+//     batched solve over all irreps (the default at these sizes) and one
+//     solve per irrep, for the Heisenberg model and the T_standard front end;
+//     the ground state kept by the batched route gives the same <Sz0 Sz1>.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -87,6 +91,29 @@ static int run() {
     HeisenbergXXZAbelianSymms_CUDA<qmb_complex> xxz(model, &T);
     const std::vector<std::vector<float>> Ex = xxz.get_E_vecs();
     expect("heisenberg_model", lowest(Ex), -5.3873909174, 2e-6);
+
+    // 7. batched route against the per-irrep route
+    {
+        qmb_dropin::irrep_route() = 2;
+        HeisenbergXXZAbelianSymms_CUDA<qmb_complex> serial(model, &T);
+        HeisenbergHamAbelianSymms_CUDA<qmb_complex> serialT(TLat, B, Jw, L / 2, &T, 9);
+        qmb_dropin::irrep_route() = 1;
+        HeisenbergXXZAbelianSymms_CUDA<qmb_complex> batched(model, &T);
+        HeisenbergHamAbelianSymms_CUDA<qmb_complex> batchedT(TLat, B, Jw, L / 2, &T, 9);
+        qmb_dropin::irrep_route() = 0;
+        const auto a = serial.get_E_vecs(), b = batched.get_E_vecs();
+        const auto at = serialT.get_E_vecs(), bt = batchedT.get_E_vecs();
+        double worst = 0.0, worst_t = 0.0;
+        for (size_t k = 0; k < a.size(); ++k) {
+            worst = std::max(worst, (double)std::fabs(a[k][0] - b[k][0]) / std::max(1.0f, std::fabs(a[k][0])));
+            worst_t = std::max(worst_t, (double)std::fabs(at[k][0] - bt[k][0]) / std::max(1.0f, std::fabs(at[k][0])));
+        }
+        expect("batched_vs_per_irrep_heisenberg", worst, 0.0, 1e-6);
+        expect("batched_vs_per_irrep_tstandard", worst_t, 0.0, 1e-6);
+        expect("batched_route_default", lowest(Ex), lowest(b), 1e-6);
+        expect("batched_route_expval_SzSz01", batched.ComputeStaticExpValZeroT(Sz<qmb_complex>(0) * Sz<qmb_complex>(1)).real(),
+               -0.1496497477, 1e-5);
+    }
 
     // 6. expectation values on the kept ground states
     Sz<qmb_complex> sz0(0), sz1(1), sz3(3);

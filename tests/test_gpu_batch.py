@@ -199,3 +199,63 @@ def test_mixed_restart_near_degenerate_pair():
     # without the gap cap 126 of the 256 starts end on the upper level, with
     # the default cap 8 did in one run
     assert (err > 1e-9).sum() <= 48, int((err > 1e-9).sum())
+
+
+@pytest.mark.parametrize("variant", range(8))
+def test_every_product_variant_matches_the_oracle(variant, monkeypatch):
+    """Each batched-product variant the tuner may choose (QMB_BHV_VARIANT
+    fixes it): one FP64 and one FP32 product on 256 coupling sets against the
+    oracle's sector matrices, and a mixed and an FP64 batched solve against
+    dense FP64 energies."""
+    import torch
+    monkeypatch.setenv("QMB_BHV_VARIANT", str(variant))
+    L, n_sets = 12, 256
+    secs, perm, ch = _sectors(L)
+    bonds = q.chain_bonds(L)
+    b = q.Batch(secs, q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"), n_sets)
+    rng = np.random.default_rng(variant)
+    J = rng.uniform(0.5, 1.5, n_sets)
+    D = rng.uniform(0.0, 2.0, n_sets)
+    E64, _ = b.solve(J, J * D, mode=A.MODE_FP64, tol=1e-12)
+    Emx, _ = b.solve(J, J * D, mode=A.MODE_MIXED, tol=1e-12)
+    assert b.info.variant_fp64 == variant and b.info.variant_fp32 == variant
+    g = oracle_group(perm, ch)
+    sec = O.build_sector(g, L // 2)
+    mats = {}
+    for a in range(L):
+        rows = O.active_rows(sec, a)
+        txy = q.xxz_terms(bonds, 1.0, 0.0)
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(txy), a, 2 * txy.n_terms + 1)
+        Mxy = O.ell_to_csr(ind, val, tr, rows)
+        tz = q.xxz_terms(bonds, 0.0, 1.0)
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(tz), a, 2 * tz.n_terms + 1)
+        mats[a] = (Mxy, O.ell_to_csr(ind, val, tr, rows))
+    for i in (0, 101, 255):
+        for a in (0, 1, L // 2, L - 1):
+            Mxy, Mz = mats[a]
+            e = O.ground_energy_dense(J[i] * Mxy + J[i] * D[i] * Mz)
+            assert abs(E64[i, a] - e) <= 1e-10 * abs(e), (i, a, E64[i, a], e)
+            assert abs(Emx[i, a] - e) <= 1e-10 * abs(e), (i, a, Emx[i, a], e)
+    off, cp = b.layout()
+    tot = int(off[-1])
+    stride = b.info.set_stride
+    for prec, dt, tol in ((A.PREC_FP64, torch.float64, 1e-12), (A.PREC_FP32, torch.float32, 2e-6)):
+        x = torch.randn(tot, dtype=dt, device="cuda", generator=torch.Generator(device="cuda").manual_seed(3))
+        y = torch.zeros_like(x)
+        b.hv_dev(x.data_ptr(), y.data_ptr(), prec)
+        torch.cuda.synchronize()
+        xs, ys = x.double().cpu().numpy(), y.double().cpu().numpy()
+        for a in (0, 1, L // 2):
+            Mxy, Mz = mats[a]
+            n = Mxy.shape[0]
+            o = int(off[a])
+            if cp[a]:
+                xv = (xs[o:o + 2 * n * stride:2] + 1j * xs[o + 1:o + 2 * n * stride:2]).reshape(n, stride)
+                yv = (ys[o:o + 2 * n * stride:2] + 1j * ys[o + 1:o + 2 * n * stride:2]).reshape(n, stride)
+            else:
+                xv = xs[o:o + n * stride].reshape(n, stride)
+                yv = ys[o:o + n * stride].reshape(n, stride)
+            for i in (0, 77, 255):
+                want = J[i] * (Mxy @ xv[:, i]) + J[i] * D[i] * (Mz @ xv[:, i])
+                np.testing.assert_allclose(yv[:, i], want, rtol=0, atol=tol * np.abs(want).max())
+    b.close()

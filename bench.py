@@ -82,8 +82,18 @@ class Clocks:
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
-            # let nvidia-smi finish starting up (its NVML initialisation)
-            # before the first timed step; sampling runs throughout
+            # wait for nvidia-smi's first samples: its NVML start-up stalls
+            # CUDA driver calls of this process for a while, which must not
+            # fall into a timed step; sampling then runs throughout
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 10.0:
+                time.sleep(0.1)
+                try:
+                    with open(self.path) as f:
+                        if sum(1 for _ in f) >= 3:
+                            break
+                except OSError:
+                    pass
             time.sleep(0.5)
         except OSError:
             self.p = None
@@ -165,6 +175,26 @@ def time_batch_hv(torch, q, b, prec, reps=20):
     e1.record(st)
     e1.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def gather_bound(q, b, hv32_ms):
+    """The batched FP32 product's x gathers against the device's bandwidth
+    for that access pattern alone (qmb_l2_gather_probe): whole x rows of all
+    sets (set stride x 8 bytes, complex FP32) read at scattered rows of a
+    buffer of one sector's rows, as many rows as the product gathers."""
+    A = q._capi
+    info = b.info
+    row_bytes = int(info.set_stride) * 8
+    rows = int(info.rows_total) // max(1, len(b.sectors))
+    gathers = int(info.nnz_total)
+    gbs, ms = A.C.c_double(), A.C.c_double()
+    q.check(q.lib().qmb_l2_gather_probe(rows, row_bytes, gathers, A.C.byref(gbs), A.C.byref(ms)))
+    kern = gathers * row_bytes / (hv32_ms * 1e-3) / 1e9
+    return {"probe": "qmb_l2_gather_probe: %d-byte rows at scattered rows of a %d-row buffer, %d gathers"
+                     % (row_bytes, rows, gathers),
+            "probe_gbs": gbs.value, "probe_ms": ms.value,
+            "k_bhv_gather_bytes": gathers * row_bytes, "k_bhv_gather_gbs": kern,
+            "k_bhv_frac_of_probe": kern / gbs.value}
 
 
 def single_sector_hv(torch, q, reps=10):
@@ -394,6 +424,8 @@ def single_sector_configs(torch, q):
     ms64, ms32 = t_hv(h, A.PREC_FP64, False, 10), t_hv(h, A.PREC_FP32, False, 10)
     mf32 = t_hv(h, A.PREC_FP32, True, 3)
     f64 = solve(h, mode=A.MODE_FP64, tol=1e-12, max_iter=300)
+    mix0 = solve(h, mode=A.MODE_MIXED, tol=1e-12, max_iter=300)
+    f64r = solve(h, mode=A.MODE_FP64, tol=1e-12, max_iter=300, reorth=2)
     mix = solve(h, mode=A.MODE_MIXED, tol=1e-12, max_iter=300, reorth=2)
     r = h.lanczos(mode=A.MODE_MIXED, tol=1e-12, max_iter=300, reorth=2, hv=A.HV_MATRIX_FREE)
     out["L32_j1j2_k0_even"] = {
@@ -403,7 +435,10 @@ def single_sector_configs(torch, q):
         "hv_ms_fp32": ms32, "hv_gbs_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9,
         "hv_frac_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9 / peak,
         "hv_ms_matrix_free_fp32": mf32,
-        "fp64": f64, "mixed_reorth2": mix, "rel_dE0": abs(mix["E0"] - f64["E0"]) / abs(f64["E0"]),
+        "fp64": f64, "mixed": mix0, "rel_dE0_no_reorth": abs(mix0["E0"] - f64["E0"]) / abs(f64["E0"]),
+        "solve_speedup_mixed_over_fp64_no_reorth": f64["ms"] / mix0["ms"],
+        "fp64_reorth2": f64r, "mixed_reorth2": mix, "rel_dE0": abs(mix["E0"] - f64r["E0"]) / abs(f64r["E0"]),
+        "solve_speedup_mixed_over_fp64_reorth2": f64r["ms"] / mix["ms"],
         "mixed_reorth2_matrix_free": {"ms": r.ms_total, "products": int(r.n_hv),
                                       "rel_dE0": abs(r.E0 - f64["E0"]) / abs(f64["E0"])}}
     h.close()
@@ -512,11 +547,13 @@ def run_batched(args, torch, q, rank, world):
         o = dict(opts, mode=mode)
         return b.solve(J, J * D, **o)
 
-    for _ in range(args.warmup):
-        solve(A.MODE_MIXED)
-    torch.cuda.synchronize()
     dev_ms, hv_count, launches = [], [], 0
+    # the clock sampler starts before the warm-up steps, so its start-up is
+    # over by the first timed step
     with Clocks(torch.cuda.current_device()) as clk:
+        for _ in range(args.warmup):
+            solve(A.MODE_MIXED)
+        torch.cuda.synchronize()
         for _ in range(args.steps):
             flush_l2(torch, flush)
             torch.cuda.synchronize()
@@ -538,6 +575,7 @@ def run_batched(args, torch, q, rank, world):
     # per-kernel H*v times
     hv32_ms = time_batch_hv(torch, q, b, A.PREC_FP32)
     hv64_ms = time_batch_hv(torch, q, b, A.PREC_FP64)
+    gather = gather_bound(q, b, hv32_ms)
     units = n_sets * L  # sector problems
     ms = float(np.mean(dev_ms))
     value = float(np.mean(hv_count)) / (ms * 1e-3)
@@ -593,6 +631,7 @@ def run_batched(args, torch, q, rank, world):
         "hv_kernel_gbs_fp32": info.bytes_hv_fp32 / (hv32_ms * 1e-3) / 1e9,
         "hv_kernel_gbs_fp64": info.bytes_hv_fp64 / (hv64_ms * 1e-3) / 1e9,
         "hv_ratio_fp32_over_fp64": hv64_ms / hv32_ms,
+        "gather_bound": gather,
         "max_rel_dE0_mixed_vs_fp64": float(rel.max()),
         "hv_tuner": {"variant_fp32": int(info.variant_fp32), "variant_fp64": int(info.variant_fp64),
                      "ms_fp32": [round(v, 4) for v in info.tune_ms_fp32],
@@ -763,6 +802,10 @@ def main():
                     help="time only the batched H*v kernels (small device footprint, for profiling)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison solve and the end-to-end repeat")
+    ap.add_argument("--profile-stored", choices=["l28", "6x6"], default=None,
+                    help="two stored FP32 products (k_hv<SellOp<float>>) on the L=28 J1-J2 k=0 even "
+                         "sector or the 6x6 k=(0,0) even sector, then exit (the launches the stored-product "
+                         "DRAM traffic summary profiles)")
     ap.add_argument("--profile-matrix-free", action="store_true",
                     help="two matrix-free FP32 products on the L=32 J1-J2 k=0 even sector, then exit "
                          "(the launch the matrix-free ncu summary profiles)")
@@ -785,6 +828,30 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import qmbcuda_b200 as q
+
+    if args.profile_stored:
+        A = q._capi
+        if args.profile_stored == "6x6":
+            N = 6
+            perm, ch = q.translation_group(N, N)
+            s = q.Sector(N * N, N * N // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+            terms = q.xxz_terms(q.square_bonds(N, N), 1.0, 1.0)
+        else:
+            L = 28
+            perm, ch = q.translation_group(L)
+            s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+            J = [1.0] * L + [0.5] * L
+            terms = q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J)
+        h = q.Hamiltonian(s, terms, prec=A.PREC_FP32)
+        x = torch.randn(int(h.info.n_rows), dtype=torch.float32, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(2):
+            q.check(q.lib().qmb_hv(h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None))
+        torch.cuda.synchronize()
+        i = h.info
+        print(json.dumps({"profile": f"stored FP32 product, {args.profile_stored}", "rows": int(i.n_rows),
+                          "nnz": int(i.nnz_offdiag), "bytes_fp32": float(i.bytes_fp32)}))
+        return 0
 
     if args.profile_matrix_free:
         A = q._capi
@@ -811,6 +878,8 @@ def main():
             print(json.dumps({"kernel": "k_bhv", "prec": "fp32" if prec == q._capi.PREC_FP32 else "fp64",
                               "ms": ms, "gbs": byt / (ms * 1e-3) / 1e9,
                               "tune_ms": list(info.tune_ms_fp32 if prec == q._capi.PREC_FP32 else info.tune_ms_fp64)}))
+            if prec == q._capi.PREC_FP32:
+                print(json.dumps({"gather_bound": gather_bound(q, b, ms)}))
         return 0
     if dist:
         dist.barrier()

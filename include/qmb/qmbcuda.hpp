@@ -11,8 +11,12 @@
  *   Lattice, T_standard<T>                             lattice_models/Lattice.h,
  *                                                      lattice_models/T_standard.h:15-34
  *   HeisenbergInfo<T>, Heisenberg<T>                   lattice_models/Heisenberg.h:10-45
+ *   CreateExtendedHeisenbergXXX, CreateHeisenbergXXXSquare,
+ *   CreateHeisenbergXXXTriangular                      lattice_models/Heisenberg.h:48-60
  *   SymmetryClass<T>, Tnm_group, Cn_group              symmetries/SymmetryClass.h:10-28,
  *                                                      symmetries/Groups.h:9-38
+ *   Iden, Cn, sigma_n_arb, Tnm, Tnm_general,
+ *   GetElemProd (as coordinate maps)                   symmetries/SymmOperators.h:5-25
  *   HeisenbergHamAbelianSymms_CUDA<T>                  exact_diagonalization/HeisenbergHamAbelianSymms_CUDA.h:17-82
  *   HeisenbergXXZAbelianSymms_CUDA<T>                  exact_diagonalization/HeisenbergGenericXXZ_AbelianSymms_CUDA.h:26-89
  *   HeisenbergHam_CUDA                                 exact_diagonalization/HeisenbergHam_CUDA.h:9-31
@@ -293,6 +297,47 @@ protected:
     int n_terms = 0;
 };
 
+// CreateExtendedHeisenbergXXX (lattice_models/Heisenberg.cu:88-176): every
+// (di, dj, a, b) coupling row of the geometry sorted by distance, J_vec[n] on
+// the n-th distance shell, the same rows and values for Jxy and Jz.
+template <typename T>
+inline Heisenberg<T> CreateExtendedHeisenbergXXX(LatticeGeometryInfo geom_info, std::vector<float> J_vec,
+                                                 bool intra_c_bool = true, bool inter_c_bool = true) {
+    if (J_vec.empty()) throw std::runtime_error("qmb: J_vec is empty");
+    qmb_dropin::Geom G = qmb_dropin::to_geom(geom_info);
+    const int M = (int)geom_info.rx_alpha.size();
+    const int cap = 4 * geom_info.N1 * geom_info.N2 * M * M;  // every candidate row
+    std::vector<double> J(J_vec.begin(), J_vec.end()), Jout((size_t)cap);
+    std::vector<int> rows(4 * (size_t)cap);
+    int n = 0;
+    qmb_dropin::check(qmb_extended_xxx_shells(&G.g, (int)J.size(), J.data(), cap, rows.data(), Jout.data(), &n));
+    HeisenbergInfo<T> hi;
+    for (int i = 0; i < n; ++i) {
+        std::vector<int> r(rows.begin() + 4 * (size_t)i, rows.begin() + 4 * (size_t)i + 4);
+        hi.Jxy_terms.push_back(r);
+        hi.Jz_terms.push_back(r);
+        hi.Jxy_couplings.push_back(qmb_dropin::make_scalar<T>::from((float)Jout[i], 0.0));
+        hi.Jz_couplings.push_back((float)Jout[i]);
+    }
+    hi.intra_c_bool = intra_c_bool;
+    hi.inter_c_bool = inter_c_bool;
+    return Heisenberg<T>(geom_info, hi);
+}
+
+// CreateHeisenbergXXXSquare / CreateHeisenbergXXXTriangular
+// (lattice_models/Heisenberg.cu:180-215): the extended XXX model on an
+// N1 x N2 square or triangular lattice.
+template <typename T>
+inline Heisenberg<T> CreateHeisenbergXXXSquare(int N1, int N2, std::vector<float> J_vec, bool intra_c_bool = true,
+                                               bool inter_c_bool = true) {
+    return CreateExtendedHeisenbergXXX<T>(create_square_lattice_info(N1, N2), J_vec, intra_c_bool, inter_c_bool);
+}
+template <typename T>
+inline Heisenberg<T> CreateHeisenbergXXXTriangular(int N1, int N2, std::vector<float> J_vec, bool intra_c_bool = true,
+                                                   bool inter_c_bool = true) {
+    return CreateExtendedHeisenbergXXX<T>(create_triangular_lattice_info(N1, N2), J_vec, intra_c_bool, inter_c_bool);
+}
+
 // ------------------------------------------------------------------ symmetry
 // A group element as a map of site coordinates: (R1, R2) -> (TR1, TR2).
 typedef std::function<void(const std::vector<float>& R1, const std::vector<float>& R2, std::vector<float>& TR1,
@@ -358,7 +403,30 @@ inline SiteMap Tnm(int Nx, int Ny, int nx, int ny) {
 // [[1, a1.a2], [a1.a2, 1]] c = (a1.r, a2.r), which takes |a1| = |a2| = 1 as
 // the reference does) are wrapped by fmod into [0, N1) x [0, N2); a
 // coefficient within 1e-3 of N counts as 0.
-inline SiteMap Tnm_general(int nx, int ny, LatticeGeometryInfo geom_info);
+inline SiteMap Tnm_general(int nx, int ny, LatticeGeometryInfo geom_info) {
+    if (geom_info.A_mat.size() != 2 || geom_info.A_mat[0].size() != 2 || geom_info.A_mat[1].size() != 2)
+        throw std::runtime_error("qmb: A_mat must be 2 x 2");
+    const double a1x = geom_info.A_mat[0][0], a1y = geom_info.A_mat[1][0];
+    const double a2x = geom_info.A_mat[0][1], a2y = geom_info.A_mat[1][1];
+    const int N1 = geom_info.N1, N2 = geom_info.N2;
+    return [=](const std::vector<float>& R1, const std::vector<float>& R2, std::vector<float>& TR1,
+               std::vector<float>& TR2) {
+        const double w = a1x * a2x + a1y * a2y;  // a1 . a2
+        const double det = 1.0 - w * w;          // Gram matrix [[1, w], [w, 1]]
+        TR1.resize(R1.size());
+        TR2.resize(R2.size());
+        for (size_t i = 0; i < R1.size(); ++i) {
+            const double x = R1[i] + nx * a1x + ny * a2x, y = R2[i] + nx * a1y + ny * a2y;
+            const double p1 = a1x * x + a1y * y, p2 = a2x * x + a2y * y;
+            double c1 = std::fmod((p1 - w * p2) / det, (double)N1);
+            double c2 = std::fmod((p2 - w * p1) / det, (double)N2);
+            if (std::fabs(c1 - N1) < 1e-3) c1 = 0.0;
+            if (std::fabs(c2 - N2) < 1e-3) c2 = 0.0;
+            TR1[i] = (float)(c1 * a1x + c2 * a2x);
+            TR2[i] = (float)(c1 * a1y + c2 * a2y);
+        }
+    };
+}
 
 // The composition G1(G2(r)), as the reference's GetElemProd
 // (symmetries/SymmOperators.cu:128-137).

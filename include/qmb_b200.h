@@ -67,6 +67,14 @@ QMB_API const char* qmb_status_string(qmb_status s);
 /* Number of visible CUDA devices (0 on a host without a GPU). */
 QMB_API int qmb_device_count(void);
 
+/* Measurement entry point, no counterpart in the reference: the current
+ * device's bandwidth (GB/s) for gathering whole rows of row_bytes bytes at
+ * scattered rows of a buffer of `rows` rows that stays in L2, the access
+ * pattern of the batched product's x gathers, with nothing else in the
+ * kernel (about `gathers` rows, kernel time in *ms, best of five launches).
+ * row_bytes is 16 times a power of two, at most 4096. */
+QMB_API qmb_status qmb_l2_gather_probe(int64_t rows, int row_bytes, int64_t gathers, double* gbs, double* ms);
+
 /* ======================================================= host-side helpers
  * Pure host code (no GPU): model and symmetry tables in reference layout. */
 
@@ -451,6 +459,7 @@ typedef struct {
     int ring_slots[2];      /* FP32 Krylov vectors the handle's ring holds now, real and
                                complex sectors (0: none yet); the ring starts at 128
                                (QMB_RING_START) and doubles when a solve needs more */
+    int64_t nnz_total;      /* off-diagonal entries of the hopping parts, all sectors */
 } qmb_batch_info;
 
 QMB_API qmb_status qmb_batch_create(const qmb_batch_desc* desc, qmb_batch* out);
@@ -462,7 +471,9 @@ QMB_API qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const double
                            const qmb_lanczos_opts* opts, double* E0, qmb_lanczos_result* summary);
 /* One batched y = H x over all pairs on device buffers in the layout of
  * qmb_batch_layout (FP64: double / complex double; FP32: float / complex
- * float).  prec: QMB_PREC_FP64 or QMB_PREC_FP32. */
+ * float).  prec: QMB_PREC_FP64 or QMB_PREC_FP32.  x_dev and y_dev must be
+ * 16-byte aligned (64-byte alignment, as cudaMalloc gives, lets the fastest
+ * kernel variants run). */
 QMB_API qmb_status qmb_batch_hv(qmb_batch b, int prec, const void* x_dev, void* y_dev, void* stream);
 /* Device vector layout: sectors of the real kind first, then those of the
  * complex kind (is_complex[s] tells which; real sectors that have fewer than

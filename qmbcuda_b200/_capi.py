@@ -91,7 +91,7 @@ class BatchInfo(C.Structure):
                 ("rows_per_block", C.c_int), ("sets_per_thread", C.c_int),
                 ("set_stride", C.c_int), ("variant_fp32", C.c_int), ("variant_fp64", C.c_int),
                 ("tune_ms_fp32", C.c_float * 8), ("tune_ms_fp64", C.c_float * 8),
-                ("ring_slots", C.c_int * 2)]
+                ("ring_slots", C.c_int * 2), ("nnz_total", C.c_int64)]
 
 
 vp = C.c_void_p
@@ -106,6 +106,7 @@ SIGNATURES = {
     "qmb_last_error": (C.c_char_p, []),
     "qmb_status_string": (C.c_char_p, [i32]),
     "qmb_device_count": (i32, []),
+    "qmb_l2_gather_probe": (i32, [i64, i32, i64, P(dbl), P(dbl)]),
     "qmb_geometry_sites": (i32, [P(Geometry), vp, vp]),
     "qmb_tstandard_pairs": (i32, [P(Geometry), i32, vp, vp, i32, i32, i32, vp, vp, vp, P(i32)]),
     "qmb_extended_xxx_shells": (i32, [P(Geometry), i32, vp, i32, vp, vp, P(i32)]),

@@ -156,7 +156,10 @@ __device__ __forceinline__ void sector_tail_reduce(const BatchArgs& a, const BLz
 //
 // HOIST: the row's own x[r] and v_{j-1}[r] are loaded before its gathers
 // instead of after them, so they travel with the first batch of gathers
-// rather than adding a dependent round trip per row.
+// rather than adding a dependent round trip per row; the per-set constants of
+// the tile (couplings, beta_j, 1/beta_j) and the alpha partials live in
+// shared memory instead of registers, which leaves the registers to the
+// gathers of the wider slices.
 template <class V, int SPL, int UNR, int MINB, bool HOIST = false>
 __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tiles, unsigned* __restrict__ ctr,
                                                    const V* __restrict__ X0, V* __restrict__ Y0,
@@ -184,6 +187,7 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tile
     const M* dz = reinterpret_cast<const M*>(a.dz);
     using R = typename Sc<V>::real;
     R cx[SPL], cz[SPL];
+    __shared__ R s_cst[HOIST ? 4 * 256 : 1];  // HOIST: cx, cz, beta_j, 1/beta_j per set (nsp <= 256)
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(ctr, 1u);
         __syncthreads();
@@ -192,10 +196,12 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tile
         if (tile >= n_tiles) break;
         const int s = a.tile_sector[tile];
         if (lanczos && !a.active[s]) continue;
+        if constexpr (!HOIST) {
 #pragma unroll
-        for (int q = 0; q < SPL; ++q) {
-            cx[q] = (R)a.cxy[(int64_t)s * a.c_stride + set0 + q];
-            cz[q] = (R)a.cz[(int64_t)s * a.c_stride + set0 + q];
+            for (int q = 0; q < SPL; ++q) {
+                cx[q] = (R)a.cxy[(int64_t)s * a.c_stride + set0 + q];
+                cz[q] = (R)a.cz[(int64_t)s * a.c_stride + set0 + q];
+            }
         }
         const int64_t nrows = a.sec_nrows[s];
         const int64_t eo = a.sec_elem[s];
@@ -206,12 +212,24 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tile
         const int prob0 = s * nsp + set0;
         R bj[SPL], inv[SPL];
         double apar[SPL];
+        if constexpr (HOIST) {
+            for (int i = threadIdx.x; i < nsp; i += blockDim.x) {
+                const double b = lanczos ? lz.beta[(int64_t)j * lz.n_prob + s * nsp + i] : 1.0;
+                s_cst[i] = (R)a.cxy[(int64_t)s * a.c_stride + i];
+                s_cst[256 + i] = (R)a.cz[(int64_t)s * a.c_stride + i];
+                s_cst[512 + i] = (R)b;
+                s_cst[768 + i] = (R)(1.0 / b);
+            }
 #pragma unroll
-        for (int q = 0; q < SPL; ++q) {
-            const double b = lanczos ? lz.beta[(int64_t)j * lz.n_prob + prob0 + q] : 1.0;
-            bj[q] = (R)b;
-            inv[q] = (R)(1.0 / b);
-            apar[q] = 0.0;
+            for (int q = 0; q < SPL; ++q) red[rg * nsp + set0 + q] = 0.0;
+        } else {
+#pragma unroll
+            for (int q = 0; q < SPL; ++q) {
+                const double b = lanczos ? lz.beta[(int64_t)j * lz.n_prob + prob0 + q] : 1.0;
+                bj[q] = (R)b;
+                inv[q] = (R)(1.0 / b);
+                apar[q] = 0.0;
+            }
         }
         const int64_t rb = a.row_base[s], d0 = a.row0[s];
         const int64_t r0 = a.tile_row0[tile];
@@ -264,18 +282,31 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tile
             const M dx = s_dx[r - r0], dzz = s_dz[r - r0];
 #pragma unroll
             for (int q = 0; q < SPL; ++q) {
-                V hx = Sc<V>::add(Sc<V>::scale(Sc<V>::fma(dx, xr.v[q], acc[q]), cx[q]),
-                                  Sc<V>::scale(Sc<V>::mul(dzz, xr.v[q]), cz[q]));
+                R cxq, czq, bjq, invq;
+                if constexpr (HOIST) {
+                    cxq = s_cst[set0 + q];
+                    czq = s_cst[256 + set0 + q];
+                    bjq = s_cst[512 + set0 + q];
+                    invq = s_cst[768 + set0 + q];
+                } else {
+                    cxq = cx[q];
+                    czq = cz[q];
+                    bjq = bj[q];
+                    invq = inv[q];
+                }
+                V hx = Sc<V>::add(Sc<V>::scale(Sc<V>::fma(dx, xr.v[q], acc[q]), cxq),
+                                  Sc<V>::scale(Sc<V>::mul(dzz, xr.v[q]), czq));
                 if (!lanczos) {
                     yo.v[q] = hx;
                     continue;
                 }
-                V vj = Sc<V>::scale(xr.v[q], inv[q]);
-                V y = Sc<V>::scale(hx, inv[q]);
-                if (j > 0) y = Sc<V>::sub(y, Sc<V>::scale(vp.v[q], bj[q]));
+                V vj = Sc<V>::scale(xr.v[q], invq);
+                V y = Sc<V>::scale(hx, invq);
+                if (j > 0) y = Sc<V>::sub(y, Sc<V>::scale(vp.v[q], bjq));
                 vo.v[q] = vj;
                 yo.v[q] = y;
-                apar[q] += Sc<V>::re_conj_mul(vj, y);
+                if constexpr (HOIST) red[rg * nsp + set0 + q] += Sc<V>::re_conj_mul(vj, y);
+                else apar[q] += Sc<V>::re_conj_mul(vj, y);
                 const double crq = (psi_v && ritz) ? ritz[(int64_t)j * lz.n_prob + prob0 + q] : 0.0;
                 if (crq != 0.0) {
                     const int64_t e = eo + r * nsp + set0 + q;
@@ -293,239 +324,10 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_bhv(BatchArgs a, int n_tile
             if (lanczos) *reinterpret_cast<PK*>(Vc + r * nsp + set0) = vo;
         }
         if (lanczos) {
+            if constexpr (!HOIST) {
 #pragma unroll
-            for (int q = 0; q < SPL; ++q) red[rg * nsp + set0 + q] = apar[q];
-            __syncthreads();
-            for (int i = threadIdx.x; i < nsp; i += blockDim.x) {
-                double tt = 0.0;
-                for (int g = 0; g < RG; ++g) tt += red[g * nsp + i];
-                lz.partials[(int64_t)tile * nsp + i] = tt;
+                for (int q = 0; q < SPL; ++q) red[rg * nsp + set0 + q] = apar[q];
             }
-            sector_tail_reduce(a, lz, s, lz.alpha + (int64_t)j * lz.n_prob, false);
-        } else {
-            __syncthreads();
-        }
-    }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned d = atomicAdd(ctr + 1, 1u);
-        if (d == gridDim.x - 1) {
-            ctr[0] = 0u;
-            ctr[1] = 0u;
-            __threadfence();
-        }
-    }
-}
-
-// Asynchronous copy of B = 4, 8 or 16 bytes global -> shared (cp.async;
-// 16-byte copies bypass L1), its commit group, and the wait for all but N of
-// this thread's groups.
-template <int B>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    if constexpr (B == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(B) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// Batched H*v / Lanczos K1 as k_bhv, with the rows of a row group flattened
-// into one stream of gather items: each row contributes its off-diagonal
-// entries x[col], then x[r] (the diagonal and v_j), then v_{j-1}[r] (Lanczos
-// steps after the first).  The tile's item list is built in shared memory
-// while the tile is staged (an item is the row index of the vector row it
-// reads; bit 31 marks a v_{j-1} row), so the next items' addresses are
-// independent loads.  Each thread copies its slices of the next stages'
-// items with cp.async into its own slots of a STAGES x UNR ring (slot
-// (stage, u) of thread t at ring[(stage * UNR + u) * blockDim + t], so a
-// warp's copies and reads are consecutive words) and consumes one stage
-// while STAGES - 1 stages are in flight: the bytes in flight are bounded by
-// shared memory rather than registers.  A thread reads only slots it filled
-// itself, so the ring needs no barrier; wait_group orders a thread's own
-// copies.  A tile's rows are split into RG contiguous runs, one per row
-// group.  Every row is computed with the same operations in the same order
-// as in k_bhv.
-template <class V, int SPL, int UNR, int STAGES, int MINB>
-__global__ void __launch_bounds__(kBThreads, MINB) k_bhv_p(BatchArgs a, int n_tiles, unsigned* __restrict__ ctr,
-                                                     const V* __restrict__ X0, V* __restrict__ Y0,
-                                                     V* __restrict__ vring, int K, BLz lz,
-                                                     const double* __restrict__ ritz, void* psi_v,
-                                                     int lanczos) {
-    static_assert(STAGES >= 2, "the ring needs two stages");
-    using M = V;
-    using PK = Pack<V, SPL>;
-    __shared__ double red[kBThreads * SPL];
-    __shared__ int s_tile;
-    __shared__ int s_rp[kBTile + 1];
-    __shared__ M s_dx[kBTile], s_dz[kBTile];
-    extern __shared__ __align__(16) unsigned char s_dyn[];
-    PK* ring = reinterpret_cast<PK*>(s_dyn);                            // [STAGES * UNR * blockDim]
-    M* s_val = reinterpret_cast<M*>(ring + STAGES * UNR * kBThreads);  // [max_tile_entries]
-    uint32_t* s_item = reinterpret_cast<uint32_t*>(s_val + a.max_tile_entries);  // [entries + 2 * kBTile]
-    const int nsp = a.nsp;
-    const int TPR = nsp / SPL;
-    const int RG = kBThreads / TPR;
-    const int rg = threadIdx.x / TPR, t = threadIdx.x % TPR, set0 = t * SPL;
-    const int j = lanczos ? *lz.iter : 0;
-    const int extra = (lanczos && j > 0) ? 2 : 1;  // items after a row's entries
-    const int64_t tot = a.sec_elem[a.n_sectors];
-    const M* val = reinterpret_cast<const M*>(a.val);
-    const M* dxy = reinterpret_cast<const M*>(a.dxy);
-    const M* dz = reinterpret_cast<const M*>(a.dz);
-    using R = typename Sc<V>::real;
-    R cx[SPL], cz[SPL];
-    PK* my = ring + threadIdx.x;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = (int)atomicAdd(ctr, 1u);
-        __syncthreads();
-        const int tile = s_tile;
-        __syncthreads();
-        if (tile >= n_tiles) break;
-        const int s = a.tile_sector[tile];
-        if (lanczos && !a.active[s]) continue;
-#pragma unroll
-        for (int q = 0; q < SPL; ++q) {
-            cx[q] = (R)a.cxy[(int64_t)s * a.c_stride + set0 + q];
-            cz[q] = (R)a.cz[(int64_t)s * a.c_stride + set0 + q];
-        }
-        const int64_t nrows = a.sec_nrows[s];
-        const int64_t eo = a.sec_elem[s];
-        const V* X = X0 + (lanczos ? (int64_t)(j & 1) * tot : 0) + eo + set0;
-        V* Y = Y0 + (lanczos ? (int64_t)((j + 1) & 1) * tot : 0) + eo;
-        V* Vc = lanczos ? vring + (int64_t)(j % K) * tot + eo : nullptr;
-        const V* Vp = lanczos ? vring + (int64_t)((j + K - 1) % K) * tot + eo + set0 : nullptr;
-        const int prob0 = s * nsp + set0;
-        R bj[SPL], inv[SPL];
-        double apar[SPL];
-#pragma unroll
-        for (int q = 0; q < SPL; ++q) {
-            const double b = lanczos ? lz.beta[(int64_t)j * lz.n_prob + prob0 + q] : 1.0;
-            bj[q] = (R)b;
-            inv[q] = (R)(1.0 / b);
-            apar[q] = 0.0;
-        }
-        const int64_t rb = a.row_base[s], d0 = a.row0[s];
-        const int64_t r0 = a.tile_row0[tile];
-        const int64_t r_end = min(nrows, r0 + kBTile);
-        const int nr = (int)(r_end - r0);
-        const int64_t e0 = a.row_ptr[rb + r0];
-        const int ne = (int)(a.row_ptr[rb + r_end] - e0);
-        for (int i = threadIdx.x; i <= nr; i += blockDim.x) s_rp[i] = (int)(a.row_ptr[rb + r0 + i] - e0);
-        for (int i = threadIdx.x; i < ne; i += blockDim.x) s_val[i] = __ldg(val + e0 + i);
-        for (int i = threadIdx.x; i < nr; i += blockDim.x) {
-            s_dx[i] = dxy[d0 + r0 + i];
-            s_dz[i] = dz[d0 + r0 + i];
-        }
-        __syncthreads();
-        // item list: row r's items start at s_rp[r] + r * extra
-        for (int i = threadIdx.x; i < ne; i += blockDim.x) {
-            int lo = 0, hi = nr;  // the row of entry i: s_rp[lo] <= i < s_rp[lo + 1]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_rp[mid] <= i) lo = mid;
-                else hi = mid;
-            }
-            s_item[i + lo * extra] = __ldg(a.col + e0 + i);
-        }
-        for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-            const int at = s_rp[r + 1] + r * extra;
-            s_item[at] = (uint32_t)(r0 + r);
-            if (extra == 2) s_item[at + 1] = (uint32_t)(r0 + r) | 0x80000000u;
-        }
-        __syncthreads();
-        const int rpg = (nr + RG - 1) / RG;
-        const int ra = min(nr, rg * rpg), rz = min(nr, ra + rpg);
-        int ii = ra < rz ? s_rp[ra] + ra * extra : 0;         // next item to issue
-        const int iend = ra < rz ? s_rp[rz] + rz * extra : 0;  // end of this group's items
-        // one stage: the next UNR items of the stream into ring stage `st`
-        auto issue = [&](int st) {
-#pragma unroll
-            for (int u = 0; u < UNR; ++u) {
-                if (ii + u < iend) {
-                    const uint32_t it = s_item[ii + u];
-                    const V* src = ((it & 0x80000000u) ? Vp : X) + (int64_t)(it & 0x7fffffffu) * nsp;
-                    cp_async<sizeof(PK)>(my + (st * UNR + u) * kBThreads, src);
-                }
-            }
-            ii += UNR;
-            cp_async_commit();
-        };
-#pragma unroll
-        for (int st = 0; st < STAGES - 1; ++st) issue(st);
-        V acc[SPL];
-#pragma unroll
-        for (int q = 0; q < SPL; ++q) acc[q] = Sc<V>::zero();
-        PK xr;
-        int cr = ra, cq = 0;  // consume cursor: row, item within the row
-        int cb = ra < rz ? s_rp[ra] : 0, cn = ra < rz ? s_rp[ra + 1] - cb : 0;
-        int st = 0;
-        while (cr < rz) {
-            cp_async_wait<STAGES - 2>();
-            // the stage consumed last round is free again
-            issue(st == 0 ? STAGES - 1 : st - 1);
-#pragma unroll
-            for (int u = 0; u < UNR; ++u) {
-                if (cr < rz) {
-                    const PK xu = my[(st * UNR + u) * kBThreads];
-                    if (cq < cn) {
-                        const M v = s_val[cb + cq];
-#pragma unroll
-                        for (int q = 0; q < SPL; ++q) acc[q] = Sc<V>::fma(v, xu.v[q], acc[q]);
-                    } else if (cq == cn) {
-                        xr = xu;
-                    }
-                    if (++cq == cn + extra) {
-                        const int64_t r = r0 + cr;
-                        const M dx = s_dx[cr], dzz = s_dz[cr];
-                        PK vo, yo;
-#pragma unroll
-                        for (int q = 0; q < SPL; ++q) {
-                            V hx = Sc<V>::add(Sc<V>::scale(Sc<V>::fma(dx, xr.v[q], acc[q]), cx[q]),
-                                              Sc<V>::scale(Sc<V>::mul(dzz, xr.v[q]), cz[q]));
-                            acc[q] = Sc<V>::zero();
-                            if (!lanczos) {
-                                yo.v[q] = hx;
-                                continue;
-                            }
-                            V vj = Sc<V>::scale(xr.v[q], inv[q]);
-                            V y = Sc<V>::scale(hx, inv[q]);
-                            if (j > 0) y = Sc<V>::sub(y, Sc<V>::scale(xu.v[q], bj[q]));
-                            vo.v[q] = vj;
-                            yo.v[q] = y;
-                            apar[q] += Sc<V>::re_conj_mul(vj, y);
-                            const double crq = (psi_v && ritz) ? ritz[(int64_t)j * lz.n_prob + prob0 + q] : 0.0;
-                            if (crq != 0.0) {
-                                const int64_t e = eo + r * nsp + set0 + q;
-                                if constexpr (Sc<V>::cplx) {
-                                    double2* p2 = reinterpret_cast<double2*>(psi_v) + e;
-                                    double2 tv = cvt<double2>(vj);
-                                    p2->x += crq * tv.x;
-                                    p2->y += crq * tv.y;
-                                } else {
-                                    reinterpret_cast<double*>(psi_v)[e] += crq * (double)vj;
-                                }
-                            }
-                        }
-                        *reinterpret_cast<PK*>(Y + r * nsp + set0) = yo;
-                        if (lanczos) *reinterpret_cast<PK*>(Vc + r * nsp + set0) = vo;
-                        cq = 0;
-                        ++cr;
-                        if (cr < rz) {
-                            cb = s_rp[cr];
-                            cn = s_rp[cr + 1] - cb;
-                        }
-                    }
-                }
-            }
-            st = st == STAGES - 1 ? 0 : st + 1;
-        }
-        cp_async_wait<0>();
-        if (lanczos) {
-#pragma unroll
-            for (int q = 0; q < SPL; ++q) red[rg * nsp + set0 + q] = apar[q];
             __syncthreads();
             for (int i = threadIdx.x; i < nsp; i += blockDim.x) {
                 double tt = 0.0;
@@ -1349,70 +1151,64 @@ static BatchArgs make_args(const qmb_batch_s* b, const BKind& k) {
 
 // Kernel variants the tuner chooses from: gathers in flight per thread
 // (UNR), the register budget (MINB resident blocks per SM), whether a row's
-// own x[r] and v_{j-1}[r] loads are hoisted ahead of its gathers (k_bhv,
-// variants 0-5), and the row group's flattened gather stream staged through
-// a shared-memory ring of STAGES x UNR slots (k_bhv_p, variants 6-7).
+// own x[r] and v_{j-1}[r] loads are hoisted ahead of its gathers, and the
+// slices per thread: one 16-byte slice of each gathered row (variants 0-2),
+// two (3-5) or four (6-7).  Wider slices mean fewer threads per row, so more
+// rows of a tile are in flight per block, and an entry's index and value
+// reads and address arithmetic serve more sets.
 constexpr int kBVariants = 8;
+constexpr int kBSlices[kBVariants] = {1, 1, 1, 2, 2, 2, 4, 4};
 
-// KIND 0: k_bhv, 1: k_bhv with hoisted row loads, 2: k_bhv_p
-template <class V, int SPL, int UNR, int MINB, int KIND, int STAGES = 2>
+template <class V, int SPL, int UNR, int MINB, bool HOIST>
 static void launch_bhv_v(const BatchArgs& a, BKind& k, const V* x, V* y, V* vring, int K, BLz lz,
                          const double* ritz, void* psi, int lanczos, cudaStream_t st) {
-    auto pick = [] {
-        if constexpr (KIND == 0) return k_bhv<V, SPL, UNR, MINB, false>;
-        else if constexpr (KIND == 1) return k_bhv<V, SPL, UNR, MINB, true>;
-        else return k_bhv_p<V, SPL, UNR, STAGES, MINB>;
-    };
-    auto kern = pick();
-    const size_t ring = KIND == 2 ? (size_t)STAGES * UNR * kBThreads * sizeof(Pack<V, SPL>) : 0;
-    const size_t items = KIND == 2 ? (size_t)(a.max_tile_entries + 2 * kBTile) * sizeof(uint32_t) : 0;
-    const size_t smem = ring + items + (size_t)a.max_tile_entries * (sizeof(V) + sizeof(uint32_t));
+    auto kern = k_bhv<V, SPL, UNR, MINB, HOIST>;
+    const size_t smem = (size_t)a.max_tile_entries * (sizeof(V) + sizeof(uint32_t));
     static int grid[64] = {0};
-    static size_t grid_smem[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     int& g = grid[dev & 63];
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (g == 0 || grid_smem[dev & 63] != smem) {
+    if (g == 0) {
         int per_sm = 0, sms = 148;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBThreads, smem);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         g = std::max(1, per_sm) * sms;
-        grid_smem[dev & 63] = smem;
     }
     g_kernels += 1;
     kern<<<std::min(g, k.n_tiles), kBThreads, smem, st>>>(a, k.n_tiles, k.d_ctr.p, x, y, vring, K, lz, ritz,
                                                           psi, lanczos);
 }
 
-// Dynamic shared memory a variant needs for this batch (the staged tile
-// entries, plus the ring and the item list of k_bhv_p).
+// Whether variant v can run this batch: a row needs at least 32 threads.
 template <class V>
-static size_t bhv_smem(int variant, const BatchArgs& a, int spl) {
-    const size_t tile = (size_t)a.max_tile_entries * (sizeof(V) + sizeof(uint32_t));
-    const size_t slot = sizeof(V) * (size_t)spl * kBThreads;
-    const size_t items = (size_t)(a.max_tile_entries + 2 * kBTile) * sizeof(uint32_t);
-    switch (variant) {
-        case 6: return tile + items + 3 * 4 * slot;
-        case 7: return tile + items + 4 * 4 * slot;
-        default: return tile;
-    }
+static bool bhv_variant_ok(int v, int nsp, int spl) {
+    const int w = kBSlices[v] * spl;
+    return w * (int)sizeof(V) <= 64 && nsp / w >= 32;
 }
 
 template <class V, int SPL>
 static void launch_bhv(int variant, const BatchArgs& a, BKind& k, const V* x, V* y, V* vring, int K,
                        BLz lz, const double* ritz, void* psi, int lanczos, cudaStream_t st) {
     if (k.n_tiles == 0) return;
+    QMB_REQUIRE(variant >= 0 && variant < kBVariants && bhv_variant_ok<V>(variant, a.nsp, SPL),
+                QMB_ERR_UNSUPPORTED, "k_bhv variant does not fit this batch's set count");
     switch (variant) {
-        case 0: launch_bhv_v<V, SPL, 8, 2, 0>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 1: launch_bhv_v<V, SPL, 8, 3, 0>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 2: launch_bhv_v<V, SPL, 4, 3, 0>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 3: launch_bhv_v<V, SPL, 4, 4, 0>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 4: launch_bhv_v<V, SPL, 4, 4, 1>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 5: launch_bhv_v<V, SPL, 8, 3, 1>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        case 6: launch_bhv_v<V, SPL, 4, 3, 2, 3>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
-        default: launch_bhv_v<V, SPL, 4, 3, 2, 4>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+        case 0: launch_bhv_v<V, SPL, 4, 4, false>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+        case 1: launch_bhv_v<V, SPL, 4, 4, true>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+        case 2: launch_bhv_v<V, SPL, 8, 2, false>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st); break;
+        default:
+            if constexpr (2 * SPL * sizeof(V) <= 64) {
+                if (variant == 3) launch_bhv_v<V, 2 * SPL, 4, 2, true>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+                else if (variant == 4) launch_bhv_v<V, 2 * SPL, 2, 3, true>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+                else if (variant == 5) launch_bhv_v<V, 2 * SPL, 2, 4, true>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+                else if constexpr (4 * SPL * sizeof(V) <= 64) {
+                    if (variant == 6) launch_bhv_v<V, 4 * SPL, 2, 2, true>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+                    else launch_bhv_v<V, 4 * SPL, 1, 2, true>(a, k, x, y, vring, K, lz, ritz, psi, lanczos, st);
+                }
+            }
+            break;
     }
 }
 
@@ -1463,7 +1259,8 @@ static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st
     // instantiation), so fixing it makes results reproducible across machines.
     if (const char* fe = std::getenv("QMB_BHV_VARIANT")) {
         const int fv = std::atoi(fe);
-        if (fe[0] >= '0' && fe[0] <= '9' && fv >= 0 && fv < kBVariants) {
+        if (fe[0] >= '0' && fe[0] <= '9' && fv >= 0 && fv < kBVariants &&
+            bhv_variant_ok<V>(fv, a.nsp, spl_for<V>(a.nsp))) {
             v = fv;
             return v;
         }
@@ -1490,14 +1287,12 @@ static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st
     QMB_CUDA_TRY(cudaEventCreate(&e1));
     // variants timed round-robin (five rounds, minimum per variant), so that
     // clock ramp-up or a one-off delay does not decide the choice
-    // variants whose shared memory exceeds the per-block limit are skipped
-    int optin = 0;
-    QMB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    // variants that cannot run this batch are skipped
     bool fits[kBVariants];
     float tmin[kBVariants];
     for (int c = 0; c < kBVariants; ++c) {
         tmin[c] = 1e30f;
-        fits[c] = bhv_smem<V>(c, a, spl_for<V>(a.nsp)) + 16 * 1024 <= (size_t)optin;
+        fits[c] = bhv_variant_ok<V>(c, a.nsp, spl_for<V>(a.nsp));
         if (fits[c]) bhv_variant<V>(c, a, k, x.p, y.p, nullptr, 1, lz, nullptr, nullptr, 0, st);  // warm
     }
     for (int r = 0; r < 5; ++r)
@@ -1730,8 +1525,20 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     ck.tile_sector.clear();
     ck.tile_row0.clear();
     ck.n_sectors = nv;
-    ck.variant[0] = k.variant[0];
-    ck.variant[1] = k.variant[1];
+    // the compacted layout has NC slots a row: a multi-slice variant that
+    // needs more sets a row gives way to the fastest one-slice variant
+    for (int f = 0; f < 2; ++f) {
+        int v = k.variant[f];
+        if (v >= 0 && kBSlices[v] > 1) {
+            int best = 0;
+            for (int c = 1; c < kBVariants; ++c)
+                if (kBSlices[c] == 1 && k.tune_ms[f][c] > 0.f &&
+                    (k.tune_ms[f][best] <= 0.f || k.tune_ms[f][c] < k.tune_ms[f][best]))
+                    best = c;
+            v = best;
+        }
+        ck.variant[f] = v;
+    }
     ck.max_tile_entries = k.max_tile_entries;
     std::vector<int64_t> rb(nv), r0(nv);
     ck.sec_elem.assign(1, 0);
@@ -2327,6 +2134,7 @@ extern "C" qmb_status qmb_batch_get_info(qmb_batch b, qmb_batch_info* info) {
             info->tune_ms_fp32[c] = kc.tune_ms[0][c];
             info->tune_ms_fp64[c] = kc.tune_ms[1][c];
         }
+        info->nnz_total = b->kind[0].nnz + b->kind[1].nnz;
         for (int kd = 0; kd < 2; ++kd) {
             const BKind& k = b->kind[kd];
             const size_t vb = (size_t)k.sec_elem.back() * (kd ? sizeof(float2) : sizeof(float));
@@ -2364,8 +2172,11 @@ static void batch_hv_kind(qmb_batch_s* b, BKind& k, bool f64, const V* x, V* y, 
     a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
     a.dz = f64 ? k.dz64.p : k.dz32.p;
     BLz lz{nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr};
-    tuned_variant<V>(a, k, f64, st);
-    bhv_any<V>(a, k, x, y, nullptr, 1, lz, nullptr, nullptr, 0, st);
+    int v = tuned_variant<V>(a, k, f64, st);
+    // the multi-slice variants read 32- or 64-byte runs: caller vectors that
+    // are only 16-byte aligned take a one-slice variant
+    if ((((uintptr_t)x | (uintptr_t)y) & 63) && kBSlices[v] > 1) v = 0;
+    bhv_variant<V>(v, a, k, x, y, nullptr, 1, lz, nullptr, nullptr, 0, st);
     check_launch("k_bhv");
 }
 }  // namespace qmb
@@ -2374,6 +2185,8 @@ extern "C" qmb_status qmb_batch_hv(qmb_batch b, int prec, const void* x_dev, voi
     return guarded([&] {
         QMB_REQUIRE(b && x_dev && y_dev, QMB_ERR_INVALID, "null argument");
         QMB_REQUIRE(prec == QMB_PREC_FP64 || prec == QMB_PREC_FP32, QMB_ERR_INVALID, "bad prec");
+        QMB_REQUIRE((((uintptr_t)x_dev | (uintptr_t)y_dev) & 15) == 0, QMB_ERR_INVALID,
+                    "x_dev and y_dev must be 16-byte aligned");
         DeviceGuard dg(b->device);
         cudaStream_t st = (cudaStream_t)stream;
         bool f64 = prec == QMB_PREC_FP64;

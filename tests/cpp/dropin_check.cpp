@@ -19,6 +19,12 @@
 //     batched solve over all irreps (the default at these sizes) and one
 //     solve per irrep, for the Heisenberg model and the T_standard front end;
 //     the ground state kept by the batched route gives the same <Sz0 Sz1>.
+//  8. solve_XXX_Heisenberg_square_generic_formalism (examples/examples.cu:
+//     885-913) as written there: the extended XXX model on the 2x4 square
+//     lattice (J1 = 1, J2 = 0.15) from CreateHeisenbergXXXSquare, the
+//     translation group of its geometry, <Sz0 Sz3>; the same model with
+//     the identity group only (union of no irreps) gives the same ground
+//     energy and correlator.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -113,6 +119,26 @@ static int run() {
         expect("batched_route_default", lowest(Ex), lowest(b), 1e-6);
         expect("batched_route_expval_SzSz01", batched.ComputeStaticExpValZeroT(Sz<qmb_complex>(0) * Sz<qmb_complex>(1)).real(),
                -0.1496497477, 1e-5);
+    }
+
+    // 8. the reference's generic-formalism example
+    {
+        Heisenberg<qmb_complex> H_model = CreateHeisenbergXXXSquare<qmb_complex>(2, 4, {1.0f, 0.15f});
+        Tnm_group symm_group(H_model.GetGeomInfo());
+        HeisenbergXXZAbelianSymms_CUDA<qmb_complex> HamG(H_model, &symm_group);
+        Operator<qmb_complex> Sz0(0, OperatorType::Sz, qmb_complex(1.0f, 0.0f));
+        Operator<qmb_complex> Sz1(3, OperatorType::Sz, qmb_complex(1.0f, 0.0f));
+        std::vector<Operator<qmb_complex>> aux_vec = {Sz0, Sz1};
+        ManyBodyOperator<qmb_complex> Sz_mb_wrapper;
+        Sz_mb_wrapper.AddTerm(aux_vec);
+        const qmb_complex Sz03 = HamG.ComputeStaticExpValZeroT(Sz_mb_wrapper);
+        SymmetryClass<qmb_complex> trivial({{qmb_complex(1.0f, 0.0f)}}, std::vector<SiteMap>{Iden});
+        HeisenbergXXZAbelianSymms_CUDA<qmb_complex> Ham1(H_model, &trivial);
+        const qmb_complex Sz03_1 = Ham1.ComputeStaticExpValZeroT(Sz_mb_wrapper);
+        std::printf("generic_formalism E0 %.10f Sz0Sz3 %.10f\n", lowest(HamG.get_E_vecs()), Sz03.real());
+        expect("generic_formalism_E0_vs_no_symmetry", lowest(HamG.get_E_vecs()), lowest(Ham1.get_E_vecs()), 2e-6);
+        expect("generic_formalism_Sz0Sz3_vs_no_symmetry", Sz03.real(), Sz03_1.real(), 1e-5);
+        expect("generic_formalism_Sz0Sz3_imag", Sz03.imag(), 0.0, 1e-6);
     }
 
     // 6. expectation values on the kept ground states

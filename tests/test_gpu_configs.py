@@ -86,3 +86,22 @@ def test_6x6_k0_even_sector_and_hermitian_hv():
     a = float(torch.dot(z.double(), hx.double()))
     b = float(torch.dot(hz.double(), x.double()))
     assert abs(a - b) <= 1e-5 * (abs(a) + abs(b))
+
+
+def test_6x6_k0_even_ground_energy():
+    """6x6 Heisenberg torus, k=(0,0), spin-inversion even: the mixed form
+    (FP32 phase, FP64 restart) and 200 fixed FP32 steps (FP64 reductions).
+    E0/36 against the published exact-diagonalisation value -0.678872
+    (Schulz, Ziman and Poilblanc, J. Phys. I France 6, 675 (1996)), which is
+    quoted to six decimals; the FP32 run agrees with the mixed one to FP32
+    level."""
+    N = 6
+    perm, ch = q.translation_group(N, N)
+    s = q.Sector(N * N, N * N // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+    h = q.Hamiltonian(s, q.xxz_terms(q.square_bonds(N, N), 1.0, 1.0), prec=A.PREC_FP32 | A.PREC_FP64)
+    rmx = h.lanczos(mode=A.MODE_MIXED, max_iter=200, tol=1e-12, refine_max_iter=200)
+    assert abs(rmx.E0 / 36 - (-0.678872)) < 1e-6, rmx.E0 / 36
+    assert rmx.residual < 1e-6 * abs(rmx.E0)
+    r32 = h.lanczos(mode=A.MODE_FP32, max_iter=200, tol=0.0, allow_unconverged=True)
+    assert r32.iters == 200
+    assert abs(r32.E0 - rmx.E0) < 1e-6 * abs(rmx.E0), (r32.E0, rmx.E0)

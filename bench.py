@@ -472,6 +472,7 @@ def single_sector_configs(torch, q):
         "hv_ms_fp32": ms32, "hv_gbs_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9,
         "hv_frac_fp32": i.bytes_fp32 / (ms32 * 1e-3) / 1e9 / peak,
         "hv_sector_gbs_fp32": gathers / (ms32 * 1e-3) / 1e9,
+        "hv_fp32_column_blocked": int(i.coded), "column_block_codes": int(i.n_codes),
         "hv_ms_fp64": ms64, "hv_gbs_fp64": i.bytes_fp64 / (ms64 * 1e-3) / 1e9,
         "hv_ms_matrix_free_fp32": mf32,
         "fp32_200_steps": fp32_200, "mixed": mixed, "fp64": fp64,
@@ -849,8 +850,17 @@ def main():
             q.check(q.lib().qmb_hv(h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None))
         torch.cuda.synchronize()
         i = h.info
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            q.check(q.lib().qmb_hv(h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None))
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 3
         print(json.dumps({"profile": f"stored FP32 product, {args.profile_stored}", "rows": int(i.n_rows),
-                          "nnz": int(i.nnz_offdiag), "bytes_fp32": float(i.bytes_fp32)}))
+                          "nnz": int(i.nnz_offdiag), "bytes_fp32": float(i.bytes_fp32),
+                          "column_blocked": int(i.coded), "ms": ms,
+                          "frac": float(i.bytes_fp32) / (ms * 1e-3) / 1e9 / load_peaks()[0]}))
         return 0
 
     if args.profile_matrix_free:
@@ -862,11 +872,18 @@ def main():
         h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J), prec=A.PREC_FP32)
         x = torch.randn(int(h.info.n_rows), dtype=torch.float32, device="cuda")
         y = torch.empty_like(x)
+        args_mf = (h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None)
         for _ in range(2):
-            q.check(q.lib().qmb_hv_matrix_free(h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()),
-                                               A.C.c_void_p(y.data_ptr()), None))
+            q.check(q.lib().qmb_hv_matrix_free(*args_mf))
         torch.cuda.synchronize()
-        print(json.dumps({"profile": "matrix-free FP32 product, L=32 J1-J2 k=0 even", "rows": int(h.info.n_rows)}))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            q.check(q.lib().qmb_hv_matrix_free(*args_mf))
+        e1.record()
+        e1.synchronize()
+        print(json.dumps({"profile": "matrix-free FP32 product, L=32 J1-J2 k=0 even", "rows": int(h.info.n_rows),
+                          "ms": e0.elapsed_time(e1) / 3}))
         return 0
 
     if args.hv_only:

@@ -111,7 +111,10 @@ __device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, 
         const bool chain = g.W == g.L;
         const uint64_t xx = ((uint64_t)x << g.L) | x;
         for (int gi = 0; gi < g.G; ++gi) {
-            const uint32_t y = chain ? (uint32_t)(xx >> (g.L - (int)sm.rot[gi].ri)) & m : apply_site_map32(g, sm, gi, x);
+            // a 32-site chain rotates by a funnel shift; shorter ones read the doubled word
+            const uint32_t y = chain ? (g.L == 32 ? __funnelshift_l(x, x, (int)sm.rot[gi].ri)
+                                                  : (uint32_t)(xx >> (g.L - (int)sm.rot[gi].ri)) & m)
+                                     : apply_site_map32(g, sm, gi, x);
             if (y < x) return false;
             if (flip && (y ^ m) < x) return false;
         }
@@ -137,7 +140,10 @@ __device__ __forceinline__ uint64_t orbit_min(const GroupArgs& g, const GroupSme
         const bool chain = g.W == g.L;
         const uint64_t xx = ((uint64_t)x << g.L) | x;
         for (int gi = 0; gi < g.G; ++gi) {
-            const uint32_t y = chain ? (uint32_t)(xx >> (g.L - (int)sm.rot[gi].ri)) & m : apply_site_map32(g, sm, gi, x);
+            // a 32-site chain rotates by a funnel shift; shorter ones read the doubled word
+            const uint32_t y = chain ? (g.L == 32 ? __funnelshift_l(x, x, (int)sm.rot[gi].ri)
+                                                  : (uint32_t)(xx >> (g.L - (int)sm.rot[gi].ri)) & m)
+                                     : apply_site_map32(g, sm, gi, x);
             if (y < best) { best = y; be = gi; }
             if (flip) {
                 const uint32_t yz = y ^ m;

@@ -11,8 +11,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <vector>
 
 #include "qmb_ham.cuh"
 
@@ -167,6 +170,7 @@ template <class Op, class V>
 void launch_hv(const Op& op, const V* x, V* y, cudaStream_t st, size_t smem) {
     const void* fn = (const void*)k_hv<Op, V>;
     set_group_smem_attr(fn, smem);
+    op.pre(x, (const int*)nullptr, st);  // earlier column-block passes, if any
     k_hv<Op, V><<<grid_for(op.n, 256), 256, smem, st>>>(op, x, y);
     check_launch("k_hv");
 }
@@ -247,6 +251,261 @@ void build_sell(qmb_ham_s* h) {
     QMB_CUDA_TRY(cudaDeviceSynchronize());
 }
 
+// ------------------------------------------ column-blocked coded layout
+constexpr int kCbMaxBlocks = 32;                     // column blocks at most
+constexpr size_t kCbBlockBytes = (size_t)64 << 20;   // x bytes of one column block
+constexpr double kCbMinVecBytes = 256.0 * (1 << 20); // vectors from this size on (2x L2)
+constexpr int kCbMissCap = 1024;                     // values outside the dictionary kept per pass
+
+// Bit pattern of a matrix value (the dictionary key).
+__device__ __forceinline__ uint64_t val_key(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ uint64_t val_key(float2 v) {
+    return ((uint64_t)__float_as_uint(v.y) << 32) | __float_as_uint(v.x);
+}
+__device__ __forceinline__ bool val_zero(float v) { return v == 0.0f; }
+__device__ __forceinline__ bool val_zero(float2 v) { return v.x == 0.0f && v.y == 0.0f; }
+
+// Every stride-th slot of the sliced ELL's FP32 values (dictionary sample).
+template <class M>
+__global__ void k_cb_sample(const M* __restrict__ val, int64_t padded, int64_t stride, int64_t n_out,
+                            uint64_t* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_out;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = i * stride;
+        out[i] = k < padded ? val_key(val[k]) : 0ull;
+    }
+}
+
+// Entries of row r (nonzero values) per column block: cnt[b * n + r].
+template <class M>
+__global__ void k_cb_count(SellOp<M> a, int shift, int nb, uint8_t* __restrict__ cnt) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = r >> 5;
+        const int lane = (int)(r & 31);
+        const int w = a.width[s];
+        int c[kCbMaxBlocks];
+        for (int b = 0; b < nb; ++b) c[b] = 0;
+        for (int j = 0; j < w; ++j) {
+            const int64_t k = a.off[s] + (int64_t)j * 32 + lane;
+            if (val_zero(a.val[k])) continue;
+            c[a.col[k] >> shift] += 1;
+        }
+        for (int b = 0; b < nb; ++b) cnt[(int64_t)b * a.n + r] = (uint8_t)c[b];
+    }
+}
+
+// Width of every (block, slice) and its slot count, slots[b * n_slices + s].
+__global__ void k_cb_width(const uint8_t* __restrict__ cnt, int64_t n, int64_t n_slices, int nb,
+                           int* __restrict__ width, int64_t* __restrict__ slots) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)nb * n_slices;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(i / n_slices);
+        const int64_t s = i % n_slices;
+        int w = 0;
+        for (int l = 0; l < 32; ++l) {
+            const int64_t r = s * 32 + l;
+            if (r < n) w = max(w, (int)cnt[(int64_t)b * n + r]);
+        }
+        width[i] = w;
+        slots[i] = (int64_t)w * 32;
+    }
+}
+
+// Packs every nonzero entry as code << 24 | column inside its block into its
+// block's slice.  A value outside the dictionary goes into the open-addressed
+// set miss_keys [kCbMissCap] (empty slots hold ~0); miss[0] counts the
+// distinct values inserted, miss[1] the ones that found no free slot.
+template <class M>
+__global__ void k_cb_fill(SellOp<M> a, int shift, int nb, const int64_t* __restrict__ off,
+                          const uint64_t* __restrict__ keys, int n_keys, uint32_t* __restrict__ packed,
+                          int* __restrict__ miss, unsigned long long* __restrict__ miss_keys) {
+    __shared__ uint64_t sk[256];
+    for (int i = threadIdx.x; i < n_keys; i += blockDim.x) sk[i] = keys[i];
+    __syncthreads();
+    const int64_t n_slices = (a.n + 31) / 32;
+    const uint32_t lmask = (1u << shift) - 1u;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = r >> 5;
+        const int lane = (int)(r & 31);
+        const int w = a.width[s];
+        int pos[kCbMaxBlocks];
+        for (int b = 0; b < nb; ++b) pos[b] = 0;
+        for (int j = 0; j < w; ++j) {
+            const int64_t k = a.off[s] + (int64_t)j * 32 + lane;
+            const M v = a.val[k];
+            if (val_zero(v)) continue;
+            const uint64_t key = val_key(v);
+            int lo = 0, hi = n_keys;  // first key >= key
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (sk[mid] < key) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo == n_keys || sk[lo] != key) {
+                uint32_t hsh = (uint32_t)(key ^ (key >> 29)) * 0x9e3779b1u;
+                int probe = 0;
+                for (; probe < kCbMissCap; ++probe) {
+                    const int at = (int)((hsh + (uint32_t)probe) & (uint32_t)(kCbMissCap - 1));
+                    const unsigned long long prev = atomicCAS(miss_keys + at, ~0ull, (unsigned long long)key);
+                    if (prev == ~0ull) atomicAdd(miss, 1);
+                    if (prev == ~0ull || prev == key) break;
+                }
+                if (probe == kCbMissCap) atomicAdd(miss + 1, 1);
+                continue;
+            }
+            const uint32_t c = a.col[k];
+            const int b = (int)(c >> shift);
+            packed[off[(int64_t)b * n_slices + s] + (int64_t)pos[b] * 32 + lane] =
+                ((uint32_t)(lo + 1) << 24) | (c & lmask);
+            pos[b] += 1;
+        }
+    }
+}
+
+// The column-blocked coded FP32 layout of a built matrix (CbSellOp), when its
+// vector is larger than L2 (at least kCbMinVecBytes), every row has fewer
+// than 256 entries, the FP32 off-diagonal values take at most 255 distinct
+// values and the layout fits in free memory.  Otherwise the handle keeps the
+// plain sliced ELL only.  QMB_COLUMN_BLOCKS=0 turns the layout off.
+// QMB_TRACE=1 says why a matrix gets no column-blocked layout.
+static void cb_skip(const char* why) {
+    const char* e = std::getenv("QMB_TRACE");
+    if (e && *e && *e != '0') std::fprintf(stderr, "[qmb ham] no column-blocked layout: %s\n", why);
+}
+
+template <class M>
+static void build_cb_t(qmb_ham_s* h, int forced_shift) {
+    const int64_t n = h->n;
+    const size_t es = sizeof(M);
+    int shift = 24;
+    while (shift > 10 && ((size_t)1 << shift) * es > kCbBlockBytes) --shift;
+    if (forced_shift) shift = forced_shift;
+    const int nb = (int)((n + ((int64_t)1 << shift) - 1) >> shift);
+    if (nb < 2 || nb > kCbMaxBlocks || h->max_row > 255) {
+        cb_skip("block count or row length out of range");
+        return;
+    }
+    SellOp<M> a = h->sell<M>(false);
+    // dictionary from a strided sample of the values
+    const int64_t n_samp = std::min<int64_t>(h->padded, (int64_t)1 << 20);
+    const int64_t stride = std::max<int64_t>(1, h->padded / n_samp);
+    std::vector<uint64_t> keys;
+    {
+        DevBuf<uint64_t> smp(n_samp);
+        k_cb_sample<M><<<grid_for(n_samp, 256), 256>>>(a.val, h->padded, stride, n_samp, smp.p);
+        check_launch("k_cb_sample");
+        std::vector<uint64_t> hs(n_samp);
+        smp.download(hs.data(), n_samp);
+        QMB_CUDA_TRY(cudaDeviceSynchronize());
+        std::sort(hs.begin(), hs.end());
+        hs.erase(std::unique(hs.begin(), hs.end()), hs.end());
+        for (uint64_t k : hs) {
+            const bool zero = es == 4 ? ((uint32_t)k << 1) == 0 : (((uint32_t)k << 1) == 0 && ((uint32_t)(k >> 32) << 1) == 0);
+            if (!zero) keys.push_back(k);
+        }
+    }
+    if (keys.empty() || keys.size() > 255) {
+        cb_skip("no values, or more than 255 distinct values in the sample");
+        return;
+    }
+    // per-block widths and offsets
+    const int64_t ns = h->n_slices;
+    size_t fr = 0, tot = 0;
+    QMB_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    if ((size_t)nb * n + 2 * n * 16 > fr / 2) {
+        cb_skip("not enough free memory for the counts");
+        return;
+    }
+    DevBuf<uint8_t> cnt((size_t)nb * n);
+    k_cb_count<M><<<grid_for(n, 256), 256>>>(a, shift, nb, cnt.p);
+    check_launch("k_cb_count");
+    DevBuf<int> width((size_t)nb * ns);
+    DevBuf<int64_t> slots((size_t)nb * ns + 1), off((size_t)nb * ns + 1);
+    QMB_CUDA_TRY(cudaMemset(slots.p + (size_t)nb * ns, 0, sizeof(int64_t)));
+    k_cb_width<<<grid_for((int64_t)nb * ns, 256), 256>>>(cnt.p, n, ns, nb, width.p, slots.p);
+    check_launch("k_cb_width");
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, slots.p, off.p, (int64_t)nb * ns + 1);
+    DevBuf<unsigned char> tmp(tb);
+    cub::DeviceScan::ExclusiveSum(tmp.p, tb, slots.p, off.p, (int64_t)nb * ns + 1);
+    int64_t total = 0;
+    QMB_CUDA_TRY(cudaMemcpy(&total, off.p + (size_t)nb * ns, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    cnt.release();
+    QMB_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    const size_t need = (size_t)total * 4 + (size_t)n * (h->cplx ? 16 : 8);
+    if (need > fr / 10 * 9) {
+        cb_skip("not enough free memory for the packed entries");
+        return;
+    }
+    DevBuf<uint32_t> packed(std::max<int64_t>(total, 1));
+    QMB_CUDA_TRY(cudaMemset(packed.p, 0, sizeof(uint32_t) * packed.n));
+    DevBuf<int> miss(2);
+    DevBuf<unsigned long long> mkeys(kCbMissCap);
+    // values the sample missed join the dictionary and the pass repeats (it
+    // rewrites every entry in place)
+    for (int round = 0;; ++round) {
+        DevBuf<uint64_t> dkeys(keys.size());
+        dkeys.upload(keys.data(), keys.size());
+        miss.zero();
+        QMB_CUDA_TRY(cudaMemset(mkeys.p, 0xff, sizeof(unsigned long long) * kCbMissCap));
+        k_cb_fill<M><<<grid_for(n, 256), 256>>>(a, shift, nb, off.p, dkeys.p, (int)keys.size(), packed.p,
+                                                miss.p, mkeys.p);
+        check_launch("k_cb_fill");
+        int hm[2] = {0, 0};
+        QMB_CUDA_TRY(cudaMemcpy(hm, miss.p, sizeof(hm), cudaMemcpyDeviceToHost));
+        if (hm[0] == 0 && hm[1] == 0) break;
+        if (hm[1] > 0 || round == 2) {
+            cb_skip("more distinct values than the dictionary holds");
+            return;
+        }
+        std::vector<unsigned long long> extra(kCbMissCap);
+        QMB_CUDA_TRY(cudaMemcpy(extra.data(), mkeys.p, sizeof(unsigned long long) * kCbMissCap,
+                                cudaMemcpyDeviceToHost));
+        for (unsigned long long k : extra)
+            if (k != ~0ull) keys.push_back(k);
+        std::sort(keys.begin(), keys.end());
+        keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+        if (keys.size() > 255) {
+            cb_skip("more than 255 distinct values");
+            return;
+        }
+    }
+    // dictionary: code 0 is the padding (value 0), code c the key c-1
+    std::vector<M> dict(256);
+    std::memset(dict.data(), 0, sizeof(M) * 256);
+    for (size_t i = 0; i < keys.size(); ++i) std::memcpy(&dict[i + 1], &keys[i], sizeof(M));
+    h->cb_dict.alloc(256 * sizeof(M));
+    QMB_CUDA_TRY(cudaMemcpy(h->cb_dict.p, dict.data(), 256 * sizeof(M), cudaMemcpyHostToDevice));
+    h->cb_ytmp.alloc((size_t)n * (h->cplx ? 16 : 8));
+    h->cb_off = std::move(off);
+    h->cb_width = std::move(width);
+    h->cb_packed = std::move(packed);
+    h->cb_nb = nb;
+    h->cb_shift = shift;
+    h->n_codes = (int)keys.size();
+    QMB_CUDA_TRY(cudaDeviceSynchronize());
+}
+
+//
+// QMB_CB_SHIFT=s (10..24) builds the layout with blocks of 2^s rows for any
+// matrix with at least two blocks, whatever its size (small cases exercise
+// the layout in tests).
+void build_cb(qmb_ham_s* h) {
+    if (!(h->prec & QMB_PREC_FP32) || !h->val32.p) return;
+    if (const char* e = std::getenv("QMB_COLUMN_BLOCKS"))
+        if (e[0] == '0') return;
+    int forced = 0;
+    if (const char* e = std::getenv("QMB_CB_SHIFT")) {
+        const int v = std::atoi(e);
+        if (v >= 10 && v <= 24) forced = v;
+    }
+    if (!forced && (double)h->n * (h->cplx ? 8 : 4) < kCbMinVecBytes) return;
+    if (h->cplx) build_cb_t<float2>(h, forced);
+    else build_cb_t<float>(h, forced);
+}
+
 }  // namespace qmb
 
 using namespace qmb;
@@ -279,6 +538,7 @@ extern "C" qmb_status qmb_ham_create(qmb_sector s, const qmb_terms* terms, int p
         h->err.alloc(1);
         h->err.zero();
         build_sell(h.get());
+        build_cb(h.get());
         if (!(prec & QMB_PREC_FP64)) {
             // keep FP64 values only when asked for; the matrix-free path needs none
             h->val64.release();
@@ -305,7 +565,7 @@ extern "C" qmb_status qmb_ham_get_info(qmb_ham h, qmb_ham_info* info) {
         info->max_row = h->max_row;
         info->is_complex = h->cplx ? 1 : 0;
         info->n_codes = h->n_codes;
-        info->coded = h->coded ? 1 : 0;
+        info->coded = h->cb_nb > 0 ? 1 : 0;
         double vs64 = h->cplx ? 16 : 8, vs32 = h->cplx ? 8 : 4;
         // compulsory traffic: index + value per off-diagonal, diagonal value,
         // x read once, y written once
@@ -390,9 +650,11 @@ void hv_dispatch(const qmb_ham_s* h, int prec, const void* x, void* y, cudaStrea
                 "the handle does not hold values of the requested precision");
     if (h->cplx) {
         if (f64) launch_hv(h->sell<double2>(true), (const double2*)x, (double2*)y, st, 0);
+        else if (h->cb_nb > 0) launch_hv(h->cb<float2>(), (const float2*)x, (float2*)y, st, CbSellOp<float2>::smem_bytes());
         else launch_hv(h->sell<float2>(false), (const float2*)x, (float2*)y, st, 0);
     } else {
         if (f64) launch_hv(h->sell<double>(true), (const double*)x, (double*)y, st, 0);
+        else if (h->cb_nb > 0) launch_hv(h->cb<float>(), (const float*)x, (float*)y, st, CbSellOp<float>::smem_bytes());
         else launch_hv(h->sell<float>(false), (const float*)x, (float*)y, st, 0);
     }
 }

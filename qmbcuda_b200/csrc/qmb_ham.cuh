@@ -143,6 +143,8 @@ struct SellOp {
     const M* diag;
     static constexpr size_t smem_bytes() { return 0; }
     __device__ void init(unsigned char*) {}
+    template <class V>
+    void pre(const V*, const int*, cudaStream_t) const {}
     // (H x)_r * scale; x_r is returned through xr.
     template <class V>
     __device__ __forceinline__ V row(int64_t r, const V* __restrict__ x, V& xr) const {
@@ -179,37 +181,49 @@ struct SellOp {
     }
 };
 
-// Packed sliced ELL: 8-bit value code in the top byte, 24-bit column below.
-template <class M>
-struct SellCodedOp {
+// Column-blocked coded sliced ELL (FP32 values), for sectors whose vector
+// is larger than L2: the columns are split into nb blocks of 2^shift rows and
+// every block has its own sliced ELL (32-row slices, column-major inside a
+// slice) whose 32-bit entries pack an 8-bit value code (into a dictionary of
+// at most 255 FP32 values; code 0 is the padding, value 0) above the 24-bit
+// column inside the block.  A product makes one pass per block in block
+// order, so the part of x a pass gathers from (one block, at most 64 MB)
+// stays in L2 while the matrix streams from HBM once: passes 0 .. nb-2
+// (pre(), k_cb_pass) leave partial row sums in ytmp, and the last pass is
+// row(), which adds its block and hands the row to the calling kernel.
+template <class M>  // float or float2
+struct CbSellOp {
     int64_t n;
-    const int64_t* off;
-    const int* width;
+    int nb;                 // column blocks
+    int shift;              // block of a column = col >> shift
+    int64_t n_slices;
+    const int64_t* off;     // [nb * n_slices] first slot of slice s in block b
+    const int* width;       // [nb * n_slices]
     const uint32_t* packed;
-    const M* dict;        // [256] in global memory, staged in shared memory
+    const M* dict;          // [256] in global memory, staged in shared memory
     const M* diag;
-    int n_codes;
+    void* ytmp;             // [n] partial sums in the product's vector type
     M* sdict;
     static constexpr size_t smem_bytes() { return 256 * sizeof(M); }
     __device__ void init(unsigned char* sm) {
         sdict = reinterpret_cast<M*>(sm);
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) sdict[i] = i < n_codes ? dict[i] : M();
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) sdict[i] = dict[i];
         __syncthreads();
     }
+    // acc + the entries of row r in column block b
     template <class V>
-    __device__ __forceinline__ V row(int64_t r, const V* __restrict__ x, V& xr) const {
-        int64_t s = r >> 5;
-        int lane = (int)(r & 31);
-        const uint32_t* p = packed + off[s] + lane;
-        int w = width[s];
-        xr = x[r];
-        V acc = Sc<V>::mul(cvt<V>(diag[r]), xr);
+    __device__ __forceinline__ V block_sum(int b, int64_t r, const V* __restrict__ x, V acc) const {
+        const int64_t s = r >> 5;
+        const int lane = (int)(r & 31);
+        const uint32_t* p = packed + off[(int64_t)b * n_slices + s] + lane;
+        const int w = width[(int64_t)b * n_slices + s];
+        const V* xb = x + ((int64_t)b << shift);
         int j = 0;
         for (; j + 4 <= w; j += 4) {
-            uint32_t p0 = __ldg(p + 0 * 32), p1 = __ldg(p + 1 * 32), p2 = __ldg(p + 2 * 32),
-                     p3 = __ldg(p + 3 * 32);
-            V x0 = __ldg(x + (p0 & 0xffffffu)), x1 = __ldg(x + (p1 & 0xffffffu)),
-              x2 = __ldg(x + (p2 & 0xffffffu)), x3 = __ldg(x + (p3 & 0xffffffu));
+            uint32_t p0 = __ldcs(p + 0 * 32), p1 = __ldcs(p + 1 * 32), p2 = __ldcs(p + 2 * 32),
+                     p3 = __ldcs(p + 3 * 32);
+            V x0 = __ldg(xb + (p0 & 0xffffffu)), x1 = __ldg(xb + (p1 & 0xffffffu)),
+              x2 = __ldg(xb + (p2 & 0xffffffu)), x3 = __ldg(xb + (p3 & 0xffffffu));
             acc = Sc<V>::fma(cvt<V>(sdict[p0 >> 24]), x0, acc);
             acc = Sc<V>::fma(cvt<V>(sdict[p1 >> 24]), x1, acc);
             acc = Sc<V>::fma(cvt<V>(sdict[p2 >> 24]), x2, acc);
@@ -217,13 +231,48 @@ struct SellCodedOp {
             p += 4 * 32;
         }
         for (; j < w; ++j) {
-            uint32_t p0 = __ldg(p);
-            acc = Sc<V>::fma(cvt<V>(sdict[p0 >> 24]), __ldg(x + (p0 & 0xffffffu)), acc);
+            uint32_t p0 = __ldcs(p);
+            acc = Sc<V>::fma(cvt<V>(sdict[p0 >> 24]), __ldg(xb + (p0 & 0xffffffu)), acc);
             p += 32;
         }
         return acc;
     }
+    // the last pass: (H x)_r from the partial sums of the earlier passes
+    template <class V>
+    __device__ __forceinline__ V row(int64_t r, const V* __restrict__ x, V& xr) const {
+        xr = x[r];
+        const V acc = nb > 1 ? reinterpret_cast<const V*>(ytmp)[r] : Sc<V>::mul(cvt<V>(diag[r]), xr);
+        return block_sum(nb - 1, r, x, acc);
+    }
+    template <class V>
+    void pre(const V* x0, const int* iter, cudaStream_t s) const;
 };
+
+// One pass of a column-blocked product: ytmp = (b == 0 ? D x : ytmp) + A_b x,
+// where x = x0, or with iter the half of the Lanczos work buffer x0 that step
+// *iter reads (as k_lz_hv does).
+template <class M, class V>
+__global__ void __launch_bounds__(256) k_cb_pass(CbSellOp<M> op, int b, const V* __restrict__ x0,
+                                                 const int* __restrict__ iter) {
+    extern __shared__ __align__(16) unsigned char smem_cb[];
+    op.init(smem_cb);
+    const V* x = x0 + (iter ? (int64_t)((*iter) & 1) * op.n : 0);
+    V* yt = reinterpret_cast<V*>(op.ytmp);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < op.n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const V acc = b == 0 ? Sc<V>::mul(cvt<V>(op.diag[r]), x[r]) : yt[r];
+        yt[r] = op.block_sum(b, r, x, acc);
+    }
+}
+
+int grid_for(int64_t n, int block);
+
+template <class M>
+template <class V>
+void CbSellOp<M>::pre(const V* x0, const int* iter, cudaStream_t s) const {
+    for (int b = 0; b + 1 < nb; ++b)
+        k_cb_pass<M, V><<<grid_for(n, 256), 256, smem_bytes(), s>>>(*this, b, x0, iter);
+}
 
 // Reference row-major ELL (caller-owned, LanczosEigVals_CUDA layout).
 template <class M>
@@ -235,6 +284,8 @@ struct RefEllOp {
     const int16_t* track;
     static constexpr size_t smem_bytes() { return 0; }
     __device__ void init(unsigned char*) {}
+    template <class V>
+    void pre(const V*, const int*, cudaStream_t) const {}
     template <class V>
     __device__ __forceinline__ V row(int64_t r, const V* __restrict__ x, V& xr) const {
         xr = x[r];
@@ -259,6 +310,8 @@ struct MfOp {
         gs = load_group(rg.g, sm);
         ts = load_terms(rg.terms, sm + align16(gbytes));
     }
+    template <class V>
+    void pre(const V*, const int*, cudaStream_t) const {}
     template <class V>
     __device__ __forceinline__ V row(int64_t r, const V* __restrict__ x, V& xr) const {
         int64_t o = rg.orbit_of_row[r];
@@ -290,10 +343,13 @@ struct qmb_ham_s {
     qmb::DevBuf<int64_t> slice_off;
     qmb::DevBuf<int> slice_w;
     qmb::DevBuf<uint32_t> col;        // plain columns
-    qmb::DevBuf<uint32_t> packed;     // code | column (when coded)
-    qmb::DevBuf<unsigned char> val64, val32, diag64, diag32, dict64, dict32;
-    int n_codes = 0;
-    bool coded = false;
+    qmb::DevBuf<unsigned char> val64, val32, diag64, diag32;
+    // column-blocked coded FP32 layout (CbSellOp), built for vectors larger than L2
+    int cb_nb = 0, cb_shift = 0, n_codes = 0;
+    qmb::DevBuf<int64_t> cb_off;
+    qmb::DevBuf<int> cb_width;
+    qmb::DevBuf<uint32_t> cb_packed;
+    qmb::DevBuf<unsigned char> cb_dict, cb_ytmp;
     // terms kept for the matrix-free operator
     int n_terms = 0, n_col = 0;
     qmb::DevBuf<int> t_nops;
@@ -336,15 +392,18 @@ struct qmb_ham_s {
         op.diag = reinterpret_cast<const M*>(fp64 ? diag64.p : diag32.p);
         return op;
     }
-    template <class M> qmb::SellCodedOp<M> sell_coded(bool fp64) const {
-        qmb::SellCodedOp<M> op;
+    template <class M> qmb::CbSellOp<M> cb() const {
+        qmb::CbSellOp<M> op;
         op.n = n;
-        op.off = slice_off.p;
-        op.width = slice_w.p;
-        op.packed = packed.p;
-        op.dict = reinterpret_cast<const M*>(fp64 ? dict64.p : dict32.p);
-        op.diag = reinterpret_cast<const M*>(fp64 ? diag64.p : diag32.p);
-        op.n_codes = n_codes;
+        op.nb = cb_nb;
+        op.shift = cb_shift;
+        op.n_slices = n_slices;
+        op.off = cb_off.p;
+        op.width = cb_width.p;
+        op.packed = cb_packed.p;
+        op.dict = reinterpret_cast<const M*>(cb_dict.p);
+        op.diag = reinterpret_cast<const M*>(diag32.p);
+        op.ytmp = cb_ytmp.p;
         op.sdict = nullptr;
         return op;
     }

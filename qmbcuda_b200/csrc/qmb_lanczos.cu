@@ -359,6 +359,7 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
     if (po.reorth) set_group_smem_attr((const void*)k_reorth_update<V>, ro_smem);
 
     auto step = [&](cudaStream_t ss) {
+        op.pre((const V*)wbuf.p, st.d.iter, ss);  // earlier column-block passes, if any
         k_lz_hv<Op, V, P><<<nb, kLzBlock, op_smem, ss>>>(op, wbuf.p, vring.p, K, st.d, nullptr,
                                                          (P*)nullptr);
         k_lz_update<V><<<nb, kLzBlock, 0, ss>>>(n, wbuf.p, vring.p, K, st.d, po.reorth ? 0 : 1);
@@ -502,6 +503,7 @@ void ritz_vector(const Op& op, size_t op_smem, const PhaseOut& ph, int start_mod
     g_lz_kernels += 2 * ph.m;  // start, m products, m - 1 updates
     k_lz_start<V, P><<<nb, kLzBlock, 0, s>>>(n, start_mode, seed, from, wbuf.p, st.d);
     for (int j = 0; j < ph.m; ++j) {
+        op.pre((const V*)wbuf.p, st.d.iter, s);
         k_lz_hv<Op, V, P><<<nb, kLzBlock, op_smem, s>>>(op, wbuf.p, vring.p, K, st.d, ritz.p, psi);
         if (j + 1 < ph.m) k_lz_update<V><<<nb, kLzBlock, 0, s>>>(n, wbuf.p, vring.p, K, st.d, 1);
         ++n_hv;
@@ -515,6 +517,7 @@ double residual_norm(const Op& op, size_t op_smem, const P* psi, double theta, L
                      cudaStream_t s, double* psi_norm2) {
     set_group_smem_attr((const void*)k_residual<Op, P>, op_smem);
     g_lz_kernels += 1;
+    op.pre(psi, (const int*)nullptr, s);
     k_residual<Op, P><<<st.nb, kLzBlock, op_smem, s>>>(op, psi, theta, st.d);
     check_launch("k_residual");
     double h[2];
@@ -720,8 +723,16 @@ extern "C" qmb_status qmb_lanczos(qmb_ham h, const qmb_lanczos_opts* opts, qmb_l
                 auto b = h->sell<double2>(true);
                 solve<SellOp<double2>, SellOp<double2>, float2, double2>(h, b, 0, b, 0, o, res, krylov_coeffs, n_coeffs);
             } else if (!need64) {
-                auto a = h->sell<float2>(false);
-                solve<SellOp<float2>, SellOp<float2>, float2, double2>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
+                if (h->cb_nb > 0) {
+                    auto a = h->cb<float2>();
+                    solve<CbSellOp<float2>, CbSellOp<float2>, float2, double2>(h, a, a.smem_bytes(), a, a.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
+                } else {
+                    auto a = h->sell<float2>(false);
+                    solve<SellOp<float2>, SellOp<float2>, float2, double2>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
+                }
+            } else if (h->cb_nb > 0) {
+                auto a = h->cb<float2>();
+                solve<CbSellOp<float2>, SellOp<double2>, float2, double2>(h, a, a.smem_bytes(), h->sell<double2>(true), 0, o, res, krylov_coeffs, n_coeffs);
             } else {
                 solve<SellOp<float2>, SellOp<double2>, float2, double2>(h, h->sell<float2>(false), 0, h->sell<double2>(true), 0, o, res, krylov_coeffs, n_coeffs);
             }
@@ -734,8 +745,16 @@ extern "C" qmb_status qmb_lanczos(qmb_ham h, const qmb_lanczos_opts* opts, qmb_l
                 auto b = h->sell<double>(true);
                 solve<SellOp<double>, SellOp<double>, float, double>(h, b, 0, b, 0, o, res, krylov_coeffs, n_coeffs);
             } else if (!need64) {
-                auto a = h->sell<float>(false);
-                solve<SellOp<float>, SellOp<float>, float, double>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
+                if (h->cb_nb > 0) {
+                    auto a = h->cb<float>();
+                    solve<CbSellOp<float>, CbSellOp<float>, float, double>(h, a, a.smem_bytes(), a, a.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
+                } else {
+                    auto a = h->sell<float>(false);
+                    solve<SellOp<float>, SellOp<float>, float, double>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
+                }
+            } else if (h->cb_nb > 0) {
+                auto a = h->cb<float>();
+                solve<CbSellOp<float>, SellOp<double>, float, double>(h, a, a.smem_bytes(), h->sell<double>(true), 0, o, res, krylov_coeffs, n_coeffs);
             } else {
                 solve<SellOp<float>, SellOp<double>, float, double>(h, h->sell<float>(false), 0, h->sell<double>(true), 0, o, res, krylov_coeffs, n_coeffs);
             }

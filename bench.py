@@ -637,8 +637,10 @@ def run_batched(args, torch, q, rank, world):
         "hv_tuner": {"variant_fp32": int(info.variant_fp32), "variant_fp64": int(info.variant_fp64),
                      "ms_fp32": [round(v, 4) for v in info.tune_ms_fp32],
                      "ms_fp64": [round(v, 4) for v in info.tune_ms_fp64],
-                     "variants": "k_bhv (unroll, min blocks/SM) = (8,2) (8,3) (4,3) (4,4); "
-                                 "k_bhv_s (streamed gathers) = (8,3) (6,4) (12,2) (16,2)"},
+                     "variants": "k_bhv (slices a thread, unroll, min blocks/SM, hoisted row loads with "
+                                 "per-set constants in shared memory): 0 (1,4,4,no) 1 (1,4,4,yes) "
+                                 "2 (1,8,2,no) 3 (2,4,2,yes) 4 (2,2,3,yes) 5 (2,2,4,yes) "
+                                 "6 (4,2,2,yes) 7 (4,1,2,yes)"},
         "e2e_with_setup": e2e_setup,
         "single_sector_hv": single,
         "observables": obs,

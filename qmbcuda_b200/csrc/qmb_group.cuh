@@ -17,6 +17,7 @@ constexpr int kTableSmemMax = 96 * 1024;
 // Group description handed to kernels by value.
 struct GroupArgs {
     int L, G, n_ext, structured, W, n_chunks;
+    int full_rot;             // a chain group of all L rotations, element 0 the identity
     uint64_t mask;
     const ElemRot* rot;       // [G] device
     const uint64_t* tables;   // [G][n_chunks][16] device
@@ -27,11 +28,12 @@ struct GroupArgs {
 struct GroupSmem {
     const ElemRot* rot;
     const uint64_t* tab;
+    const int* gofr;  // full_rot: the element of each rotation amount
 };
 
 // Bytes of dynamic shared memory a kernel needs for the group.
 __host__ __device__ inline size_t group_smem_bytes(const GroupArgs& g) {
-    if (g.structured) return sizeof(ElemRot) * (size_t)g.G;
+    if (g.structured) return sizeof(ElemRot) * (size_t)g.G + sizeof(int) * 64;
     size_t t = sizeof(uint64_t) * (size_t)g.G * g.n_chunks * 16;
     return t <= (size_t)kTableSmemMax ? t : 0;
 }
@@ -39,11 +41,17 @@ __host__ __device__ inline size_t group_smem_bytes(const GroupArgs& g) {
 // Cooperative load of the group into dynamic shared memory `sm`.
 __device__ __forceinline__ GroupSmem load_group(const GroupArgs& g, unsigned char* sm) {
     GroupSmem out;
+    out.gofr = nullptr;
     if (g.structured) {
         ElemRot* r = reinterpret_cast<ElemRot*>(sm);
-        for (int i = threadIdx.x; i < g.G; i += blockDim.x) r[i] = g.rot[i];
+        int* gofr = reinterpret_cast<int*>(r + g.G);
+        for (int i = threadIdx.x; i < g.G; i += blockDim.x) {
+            r[i] = g.rot[i];
+            if (g.full_rot) gofr[g.rot[i].ri] = i;
+        }
         out.rot = r;
         out.tab = g.tables;
+        out.gofr = gofr;
     } else {
         size_t n = (size_t)g.G * g.n_chunks * 16;
         if (n * sizeof(uint64_t) <= (size_t)kTableSmemMax) {
@@ -102,8 +110,15 @@ __device__ __forceinline__ uint32_t apply_site_map32(const GroupArgs& g, const G
     return rot32_rows(rot32_bits(s, (int)e.rr, g.L, (uint32_t)g.mask), (int)e.ri, g.W, (uint32_t)e.lo);
 }
 
+__device__ __forceinline__ uint32_t chain_orbit_min(const GroupArgs& g, const GroupSmem& sm, uint32_t x,
+                                                    int* elem);
+
 // True iff no element maps s below s (s is its orbit's minimum).
 __device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, uint64_t s) {
+    if (g.full_rot) {
+        int e;
+        return chain_orbit_min(g, sm, (uint32_t)s, &e) == (uint32_t)s;
+    }
     if (g.structured && g.L <= 32) {
         const uint32_t x = (uint32_t)s, m = (uint32_t)g.mask;
         const bool flip = g.n_ext > g.G;
@@ -128,9 +143,81 @@ __device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, 
     return true;
 }
 
+// The orbit minimum of x under all L rotations of a chain (and, with flip,
+// their complements), and the first element reaching it in the (element,
+// inversion) order of orbit_min's loop.  A rotation's leading zeros are a run
+// of zeros of the string, so the minimum brings the top of a longest run of
+// zeros (bit p zero, bit p+1 one, cyclically) to bit L-1, and every rotation
+// reaching it does.  The tops are filtered down to those of the longest runs
+// (one AND a step, as many steps as the longest run is long), and only those
+// rotations are compared: usually one or two instead of L, or 2L with flip.
+__device__ __forceinline__ uint32_t rotl_chain(uint32_t v, int r, int L, uint32_t m) {
+    return L == 32 ? __funnelshift_l(v, v, r) : (r ? (((v << r) | (v >> (L - r))) & m) : v);
+}
+
+__device__ __forceinline__ uint32_t chain_orbit_min(const GroupArgs& g, const GroupSmem& sm, uint32_t x,
+                                                    int* elem) {
+    const int L = g.L;
+    const uint32_t m = (uint32_t)g.mask;
+    const int nz = g.n_ext > g.G ? 2 : 1;
+    uint32_t tops[2] = {0u, 0u};
+    int run[2] = {-1, -1};
+#pragma unroll
+    for (int z = 0; z < 2; ++z) {
+        if (z >= nz) break;
+        const uint32_t v = z ? (~x & m) : x;
+        const uint32_t zeros = ~v & m;
+        uint32_t c = zeros & rotl_chain(v, L - 1, L, m);  // bit p zero, bit p+1 one
+        if (!c) {  // constant string
+            run[z] = v ? 0 : L;
+            continue;
+        }
+        int k = 1;
+        uint32_t below = zeros;
+        for (;;) {
+            below = rotl_chain(below, 1, L, m);  // bit p: zero k bits below p
+            const uint32_t nx = c & below;
+            if (!nx) break;
+            c = nx;
+            ++k;
+        }
+        tops[z] = c;
+        run[z] = k;
+    }
+    const int longest = max(run[0], run[1]);
+    uint32_t best = x;  // element 0, the identity
+    int bg = 0, bz = 0;
+#pragma unroll
+    for (int z = 0; z < 2; ++z) {
+        if (z >= nz || run[z] != longest) continue;
+        const uint32_t v = z ? (~x & m) : x;
+        uint32_t c = tops[z];
+        if (!c && v < best) {  // constant: every rotation gives v, element 0 first
+            best = v;
+            bg = 0;
+            bz = z;
+        }
+        while (c) {
+            const int p = __ffs(c) - 1;
+            c &= c - 1;
+            const int r = L - 1 - p;
+            const uint32_t y = rotl_chain(v, r, L, m);
+            const int gi = sm.gofr[r];
+            if (y < best || (y == best && (gi < bg || (gi == bg && z < bz)))) {
+                best = y;
+                bg = gi;
+                bz = z;
+            }
+        }
+    }
+    *elem = bz ? bg + g.G : bg;
+    return best;
+}
+
 // Minimum of the orbit of t and the first element reaching it.
 __device__ __forceinline__ uint64_t orbit_min(const GroupArgs& g, const GroupSmem& sm, uint64_t t,
                                               int* elem) {
+    if (g.full_rot) return chain_orbit_min(g, sm, (uint32_t)t, elem);
     if (g.structured && g.L <= 32) {
         const uint32_t x = (uint32_t)t, m = (uint32_t)g.mask;
         const bool flip = g.n_ext > g.G;

@@ -21,6 +21,56 @@
 
 namespace qmb {
 
+// The hop form of a validated term table (MfOp): every term either diagonal
+// (SZ and identity operators) or one SP and one SM at two distinct sites with
+// nothing else; otherwise n_hops = 0 and the operator runs the general term
+// loop.  Hops on the same two sites merge, per direction.
+static void hop_form(qmb_ham_s* h, const qmb_terms* t) {
+    h->n_hops = 0;
+    std::vector<Hop> hp;
+    std::vector<double2> cf;
+    for (int i = 0; i < t->n_terms; ++i) {
+        int sp = -1, sm = -1, n_sz = 0, n_other = 0;
+        for (int j = 0; j < t->n_ops[i]; ++j) {
+            const int c = t->op_code[i * t->n_col + j], st = t->op_site[i * t->n_col + j];
+            if (c == QMB_OP_SP) {
+                if (sp >= 0) ++n_other;
+                sp = st;
+            } else if (c == QMB_OP_SM) {
+                if (sm >= 0) ++n_other;
+                sm = st;
+            } else if (c == QMB_OP_SZ) {
+                ++n_sz;
+            }
+        }
+        if (sp < 0 && sm < 0) continue;  // diagonal
+        if (sp < 0 || sm < 0 || sp == sm || n_sz || n_other) return;
+        const int a = std::min(sp, sm), b = std::max(sp, sm);
+        const uint64_t pair = (1ull << a) | (1ull << b);
+        size_t k = 0;
+        while (k < hp.size() && hp[k].pair != pair) ++k;
+        if (k == hp.size()) {
+            if ((int)hp.size() == kMaxHops) return;
+            hp.push_back(Hop{pair});
+            cf.push_back(make_double2(0.0, 0.0));
+            cf.push_back(make_double2(0.0, 0.0));
+        }
+        // raising the lower site a (bit a zero, bit b one) is direction 0
+        double2& c = cf[2 * k + (sp == a ? 0 : 1)];
+        c.x += t->scalar[2 * i];
+        c.y += t->scalar[2 * i + 1];
+    }
+    if (hp.empty()) return;
+    h->hop_one_way = 0;
+    for (const double2& c : cf)
+        if (c.x == 0.0 && c.y == 0.0) h->hop_one_way = 1;
+    h->hops.alloc(hp.size());
+    h->hops.upload(hp.data(), hp.size());
+    h->hop_c.alloc(cf.size());
+    h->hop_c.upload(cf.data(), cf.size());
+    h->n_hops = (int)hp.size();
+}
+
 void upload_terms(qmb_ham_s* h, const qmb_terms* t, int L) {
     QMB_REQUIRE(t && t->n_ops && t->op_code && t->op_site && t->scalar, QMB_ERR_INVALID,
                 "terms: null table");
@@ -45,6 +95,7 @@ void upload_terms(qmb_ham_s* h, const qmb_terms* t, int L) {
         QMB_REQUIRE(std::isfinite(sc[i].x) && std::isfinite(sc[i].y), QMB_ERR_INVALID,
                     "terms: non-finite scalar");
     }
+    hop_form(h, t);
     h->n_terms = t->n_terms;
     h->n_col = t->n_col;
     h->t_nops.alloc(std::max(1, t->n_terms));
@@ -148,7 +199,7 @@ __global__ void k_ell_ref(RowGen rg, int64_t R, int W, uint32_t* __restrict__ in
 }
 
 template <class Op, class V>
-__global__ void k_hv(Op op, const V* __restrict__ x, V* __restrict__ y) {
+__global__ void __launch_bounds__(256, OpMinBlocks<Op>::value) k_hv(Op op, const V* __restrict__ x, V* __restrict__ y) {
     extern __shared__ __align__(16) unsigned char smem_hv[];
     op.init(smem_hv);
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < op.n;
@@ -170,7 +221,7 @@ template <class Op, class V>
 void launch_hv(const Op& op, const V* x, V* y, cudaStream_t st, size_t smem) {
     const void* fn = (const void*)k_hv<Op, V>;
     set_group_smem_attr(fn, smem);
-    op.pre(x, (const int*)nullptr, st);  // earlier column-block passes, if any
+    op.pre(x, (const int*)nullptr, st);  // column-block passes or the matrix-free scaling, if any
     k_hv<Op, V><<<grid_for(op.n, 256), 256, smem, st>>>(op, x, y);
     check_launch("k_hv");
 }
@@ -506,6 +557,100 @@ void build_cb(qmb_ham_s* h) {
     else build_cb_t<float>(h, forced);
 }
 
+// Row-order copies for the matrix-free lookup: each row's representative
+// (32-bit, 64-bit or neither) and its orbit's norm.
+__global__ void k_mf_rows(int64_t n, const int64_t* __restrict__ orbit_of_row, const uint64_t* __restrict__ reps,
+                          const double* __restrict__ norms, uint32_t* __restrict__ reps32,
+                          uint64_t* __restrict__ reps64, double* __restrict__ nrow) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = orbit_of_row[r];
+        nrow[r] = norms[o];
+        if (reps32) reps32[r] = (uint32_t)reps[o];
+        if (reps64) reps64[r] = reps[o];
+    }
+}
+
+// bucket[b] = first row whose representative's top bits are >= b.
+template <class K>
+__global__ void k_mf_bucket(const K* __restrict__ reps, int64_t n, int shift, uint64_t n_b,
+                            uint32_t* __restrict__ bucket) {
+    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b <= n_b;
+         b += (uint64_t)gridDim.x * blockDim.x) {
+        if (b == n_b) {
+            bucket[b] = (uint32_t)n;
+            continue;
+        }
+        const uint64_t key = b << shift;
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((uint64_t)reps[mid] < key) lo = mid + 1;
+            else hi = mid;
+        }
+        bucket[b] = (uint32_t)lo;
+    }
+}
+
+// The stored diagonal of the hop form.
+template <class D>
+__global__ void k_mf_diag(RowGen rg, int64_t n, D* __restrict__ diag) {
+    QMB_LOAD_GEN(rg);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t src = apply_elem(rg.g, gs, 0, rg.rt.reps[rg.orbit_of_row[r]]);
+        const double2 d = row_diagonal(ts, src);
+        if constexpr (sizeof(D) == sizeof(double2)) diag[r] = d;
+        else diag[r] = d.x;
+    }
+}
+
+// The matrix-free operator's tables.  The rows' representatives in row
+// order (32-bit up to 32 sites; beyond, the sector's table when every orbit
+// is active), the bucket table over them on the top 24 bits of the largest
+// one, the rows' norms, the diagonal of the hop form and the xs buffer.
+void mf_tables(qmb_ham_s* h) {
+    if (h->mf_ready) return;
+    qmb_sector_s* s = h->sector;
+    const int64_t n = h->n;
+    const bool all = s->n_active == s->R;
+    const bool r32 = s->L <= 32;
+    h->mf_norm.alloc(n);
+    if (r32) h->mf_reps32.alloc(n);
+    else if (!all) h->mf_reps64.alloc(n);
+    k_mf_rows<<<grid_for(n, 256), 256>>>(n, s->orbit_of_row.p, s->reps.p, s->norms.p, h->mf_reps32.p,
+                                         h->mf_reps64.p, h->mf_norm.p);
+    check_launch("k_mf_rows");
+    int64_t o_last = 0;  // rows ascend with their representatives: the last is the largest
+    uint64_t top = 0;
+    QMB_CUDA_TRY(cudaMemcpy(&o_last, s->orbit_of_row.p + (n - 1), sizeof(int64_t), cudaMemcpyDeviceToHost));
+    QMB_CUDA_TRY(cudaMemcpy(&top, s->reps.p + o_last, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    int bits = 0;
+    while (bits < 64 && (top >> bits)) ++bits;
+    h->mf_shift = std::max(0, bits - 24);
+    h->mf_nb = (top >> h->mf_shift) + 1;
+    h->mf_bucket.alloc(h->mf_nb + 1);
+    const int g = grid_for((int64_t)h->mf_nb + 1, 256);
+    if (r32) k_mf_bucket<uint32_t><<<g, 256>>>(h->mf_reps32.p, n, h->mf_shift, h->mf_nb, h->mf_bucket.p);
+    else k_mf_bucket<uint64_t><<<g, 256>>>(all ? s->reps.p : h->mf_reps64.p, n, h->mf_shift, h->mf_nb,
+                                              h->mf_bucket.p);
+    check_launch("k_mf_bucket");
+    if (h->n_hops) {
+        const RowGen rg = h->row_gen();
+        const size_t sm = gen_smem(rg);
+        h->mf_diag.alloc((size_t)n * (h->cplx ? 16 : 8));
+        if (h->cplx) {
+            set_group_smem_attr((const void*)k_mf_diag<double2>, sm);
+            k_mf_diag<double2><<<grid_for(n, 128), 128, sm>>>(rg, n, reinterpret_cast<double2*>(h->mf_diag.p));
+        } else {
+            set_group_smem_attr((const void*)k_mf_diag<double>, sm);
+            k_mf_diag<double><<<grid_for(n, 128), 128, sm>>>(rg, n, reinterpret_cast<double*>(h->mf_diag.p));
+        }
+        check_launch("k_mf_diag");
+    }
+    h->mf_xs.alloc((size_t)n * (h->cplx ? 16 : 8));
+    QMB_CUDA_TRY(cudaDeviceSynchronize());
+    h->mf_ready = true;
+}
+
 }  // namespace qmb
 
 using namespace qmb;
@@ -673,6 +818,7 @@ extern "C" qmb_status qmb_hv_matrix_free(qmb_ham h, int prec, const void* x_dev,
     return guarded([&] {
         QMB_REQUIRE(h && x_dev && y_dev, QMB_ERR_INVALID, "null argument");
         DeviceGuard dg(h->device);
+        mf_tables(h);
         hv_dispatch(h, prec, x_dev, y_dev, (cudaStream_t)stream, true);
     });
 }

@@ -65,36 +65,78 @@ struct RowGen {
 };
 
 
-// Enumerates the entries of the row whose source string is src (norm ns)
-// generated by terms h0 .. h1-1: emit(orbit, value) for every off-diagonal
-// entry, the diagonal is returned.
+// Term hi applied to the basis string src: false when an operator
+// annihilates it, else the image *t and the coefficient *coef.  Ops act from
+// the first column on; codes other than SZ, SP and SM act as the identity.
+__device__ __forceinline__ bool apply_term(const TermsSmem& ts, int hi, uint64_t src, uint64_t* t_out,
+                                           double2* coef_out) {
+    uint64_t t = src;
+    double2 coef = ts.scalar[hi];
+    const uint16_t* op = ts.ops + hi * ts.n_col;
+    for (int h2 = 0; h2 < ts.n_ops[hi]; ++h2) {
+        const int code = op[h2] >> 8, site = op[h2] & 0xff;
+        const int spin = (int)((t >> site) & 1ull);
+        if (code == QMB_OP_SM) {
+            if (!spin) return false;
+            t &= ~(1ull << site);
+        } else if (code == QMB_OP_SP) {
+            if (spin) return false;
+            t |= 1ull << site;
+        } else if (code == QMB_OP_SZ) {
+            const double f = spin ? 0.5 : -0.5;
+            coef.x *= f;
+            coef.y *= f;
+        }
+    }
+    *t_out = t;
+    *coef_out = coef;
+    return true;
+}
+
+// The diagonal element of the row of src: the terms that map src to itself.
+__device__ __forceinline__ double2 row_diagonal(const TermsSmem& ts, uint64_t src) {
+    double2 d = make_double2(0.0, 0.0);
+    for (int hi = 0; hi < ts.n_terms; ++hi) {
+        uint64_t t;
+        double2 coef;
+        if (apply_term(ts, hi, src, &t, &coef) && t == src) {
+            d.x += coef.x;
+            d.y += coef.y;
+        }
+    }
+    return d;
+}
+
+// Where gen_row_look finds a generated representative r: the sector's orbit
+// table, each entry scaled by n(target) / n(source).  find() returns 1 with
+// the orbit and the factor, 0 for a null orbit (the entry is dropped), -1
+// when r is not in the sector.
+struct OrbitLookup {
+    double ns;
+    __device__ __forceinline__ int find(const RowGen& rg, uint64_t r, int64_t* idx, double* f) const {
+        const int64_t o = find_rep(rg.rt, r);
+        if (o < 0) return -1;
+        const double nt = rg.norms[o];
+        if (nt < rg.tol) return 0;
+        *idx = o;
+        *f = nt / ns;
+        return 1;
+    }
+};
+
+// Enumerates the entries of the row whose source string is src generated by
+// terms h0 .. h1-1: emit(index, value) for every off-diagonal entry, with the
+// index and the norm factor from look.find(); the diagonal is returned.
 // Rule of BuildHamiltonianXXZForAbelianGroup (exact_diagonalization/utils.cu:83-184).
-template <class Emit>
-__device__ __forceinline__ double2 gen_row_range(const RowGen& rg, const GroupSmem& gs,
-                                                 const TermsSmem& ts, int h0, int h1, uint64_t src,
-                                                 double ns, Emit&& emit) {
+template <class Look, class Emit>
+__device__ __forceinline__ double2 gen_row_look(const RowGen& rg, const GroupSmem& gs,
+                                                const TermsSmem& ts, int h0, int h1, uint64_t src,
+                                                const Look& look, Emit&& emit) {
     double2 diag = make_double2(0.0, 0.0);
     for (int hi = h0; hi < h1; ++hi) {
-        uint64_t t = src;
-        double2 coef = ts.scalar[hi];
-        bool bad = false;
-        const uint16_t* op = ts.ops + hi * ts.n_col;
-        for (int h2 = 0; h2 < ts.n_ops[hi]; ++h2) {
-            int code = op[h2] >> 8, site = op[h2] & 0xff;
-            int spin = (int)((t >> site) & 1ull);
-            if (code == QMB_OP_SM) {
-                if (!spin) { bad = true; break; }
-                t &= ~(1ull << site);
-            } else if (code == QMB_OP_SP) {
-                if (spin) { bad = true; break; }
-                t |= 1ull << site;
-            } else if (code == QMB_OP_SZ) {
-                double f = spin ? 0.5 : -0.5;
-                coef.x *= f;
-                coef.y *= f;
-            }
-        }
-        if (bad) continue;
+        uint64_t t;
+        double2 coef;
+        if (!apply_term(ts, hi, src, &t, &coef)) continue;
         if (t == src) {
             diag.x += coef.x;
             diag.y += coef.y;
@@ -105,22 +147,31 @@ __device__ __forceinline__ double2 gen_row_range(const RowGen& rg, const GroupSm
             continue;
         }
         int e;
-        uint64_t r = orbit_min(rg.g, gs, t, &e);
-        int64_t o = find_rep(rg.rt, r);
-        if (o < 0) {
+        const uint64_t r = orbit_min(rg.g, gs, t, &e);
+        int64_t o;
+        double f;
+        const int found = look.find(rg, r, &o, &f);
+        if (found < 0) {
             *rg.err = 2;
             continue;
         }
-        double nt = rg.norms[o];
-        if (nt < rg.tol) continue;
+        if (!found) continue;
         // t = g_e^{-1}(rep): chi(g_t) = conj(chi(e)) for a unitary 1-D irrep
         double2 ch = rg.g.chars[e];
-        double f = nt / ns;
         double2 v = make_double2((coef.x * ch.x + coef.y * ch.y) * f,
                                  (coef.y * ch.x - coef.x * ch.y) * f);
         emit(o, v);
     }
     return diag;
+}
+
+// gen_row_look over the sector's orbit table: emit(orbit, value), the source
+// orbit's norm ns.
+template <class Emit>
+__device__ __forceinline__ double2 gen_row_range(const RowGen& rg, const GroupSmem& gs,
+                                                 const TermsSmem& ts, int h0, int h1, uint64_t src,
+                                                 double ns, Emit&& emit) {
+    return gen_row_look(rg, gs, ts, h0, h1, src, OrbitLookup{ns}, static_cast<Emit&&>(emit));
 }
 
 // All terms of the table.
@@ -297,36 +348,230 @@ struct RefEllOp {
     }
 };
 
-// Matrix-free operator: regenerates every entry of the row.
+// The matrix-free operator's lookup: the representatives of the active
+// orbits in row order (ascending), 32-bit when L <= 32, with a bucket table on
+// their top bits, so a generated representative maps straight to its row.
+// The norm factor is left out (f = 1): the operator gathers n(c) x_c and
+// divides the row by its own norm.
+struct ActiveLookup {
+    const uint32_t* reps32;  // [n] or null
+    const uint64_t* reps64;  // [n] when reps32 is null
+    const uint32_t* bucket;  // [n_b + 1]: rows of bucket b (top bits r >> shift == b)
+    int shift;               // the largest representative's bit length - 24, at least 0
+    uint64_t n_b;
+    int64_t n;
+    int all_active;          // every orbit is a row: a miss is outside the sector
+    __device__ __forceinline__ int find(const RowGen& rg, uint64_t r, int64_t* idx, double* f) const {
+        const uint64_t b = r >> shift;
+        int64_t lo = 0, hi = 0;
+        if (b < n_b) {
+            lo = bucket[b];
+            hi = bucket[b + 1];
+        }
+        bool hit;
+        if (reps32) {
+            const uint32_t k = (uint32_t)r;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (__ldg(reps32 + mid) < k) lo = mid + 1;
+                else hi = mid;
+            }
+            hit = lo < n && __ldg(reps32 + lo) == k;
+        } else {
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (__ldg(reps64 + mid) < r) lo = mid + 1;
+                else hi = mid;
+            }
+            hit = lo < n && __ldg(reps64 + lo) == r;
+        }
+        if (hit) {
+            *idx = lo;
+            *f = 1.0;
+            return 1;
+        }
+        if (all_active) return -1;
+        return find_rep(rg.rt, r) < 0 ? -1 : 0;  // a null orbit, or outside the sector
+    }
+    // find() for L <= 32 (reps32 set), in 32-bit arithmetic
+    __device__ __forceinline__ int find32(const RowGen& rg, uint32_t r, uint32_t* idx) const {
+        const uint32_t b = r >> shift;
+        uint32_t lo = 0, hi = 0;
+        if (b < (uint32_t)n_b) {
+            lo = bucket[b];
+            hi = bucket[b + 1];
+        }
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo) >> 1);
+            if (__ldg(reps32 + mid) < r) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < (uint32_t)n && __ldg(reps32 + lo) == r) {
+            *idx = lo;
+            return 1;
+        }
+        if (all_active) return -1;
+        return find_rep(rg.rt, r) < 0 ? -1 : 0;
+    }
+};
+
+// Two-site exchange ("hop") form of a term table, for the matrix-free
+// operator: every off-diagonal term is c S+_i S-_j at two distinct sites and
+// every other term is diagonal (SZ and identity operators only).  Hops on the
+// same pair of sites are merged into one entry with the coefficient of each
+// direction.
+constexpr int kMaxHops = 512;
+struct Hop {
+    uint64_t pair;  // bits i < j; direction 0 raises site i (bit i zero, bit j one)
+};
+
+// Matrix-free operator: regenerates every entry of the row.  pre() writes
+// xs = n(c) x_c; a row then sums the unscaled entries times xs and divides by
+// its own norm, so the only data a generated entry gathers are the active
+// representatives it searches and one element of xs (together 8 bytes a row
+// at L <= 32 in FP32: 75 MB at L = 32, inside L2).
+//
+// With a hop table (n_hops > 0) the diagonal comes from the stored vector
+// diag and the entries of a row are the hops whose two sites differ in the
+// source string: a 64-bit mask of them (per 64 hops) is formed first and its
+// set bits are walked, so the threads of a warp run the orbit search and the
+// lookup together instead of at the term where each finds an entry.  Up to
+// 32 sites the strings, masks, representatives and row indices are 32-bit.
 template <class M>
 struct MfOp {
     int64_t n;
     RowGen rg;
+    ActiveLookup look;
+    const double* nrow;  // [n] norm of each row's orbit
+    void* xs;            // [n] scaled x in the product's vector type
+    int n_hops;
+    int hop_one_way;     // some hop has a zero coefficient in one direction
+    const Hop* hops;     // [n_hops]
+    const double2* hop_c;  // [2 n_hops]: coefficient for bit i = 0, bit j = 1; then the reverse
+    const void* diag;    // [n] the diagonal (double2 for complex handles, else double)
+    int cplx;
     GroupSmem gs;
     TermsSmem ts;
+    const Hop* s_hops;
+    const uint32_t* s_pair32;  // low words of the pairs
+    const double2* s_hop_c;
     size_t gbytes;
-    size_t smem_bytes() const { return align16(gbytes) + terms_smem_bytes(rg.terms); }
+    size_t smem_bytes() const {
+        return align16(gbytes) + (n_hops ? (sizeof(Hop) + 2 * sizeof(double2) + sizeof(uint32_t)) * (size_t)n_hops
+                                         : terms_smem_bytes(rg.terms));
+    }
     __device__ void init(unsigned char* sm) {
         gs = load_group(rg.g, sm);
-        ts = load_terms(rg.terms, sm + align16(gbytes));
+        if (n_hops) {
+            double2* c = reinterpret_cast<double2*>(sm + align16(gbytes));
+            Hop* hp = reinterpret_cast<Hop*>(c + 2 * n_hops);
+            uint32_t* p32 = reinterpret_cast<uint32_t*>(hp + n_hops);
+            for (int i = threadIdx.x; i < n_hops; i += blockDim.x) {
+                hp[i] = hops[i];
+                p32[i] = (uint32_t)hops[i].pair;
+                c[2 * i] = hop_c[2 * i];
+                c[2 * i + 1] = hop_c[2 * i + 1];
+            }
+            s_hops = hp;
+            s_pair32 = p32;
+            s_hop_c = c;
+            __syncthreads();
+        } else {
+            ts = load_terms(rg.terms, sm + align16(gbytes));
+        }
     }
     template <class V>
-    void pre(const V*, const int*, cudaStream_t) const {}
+    void pre(const V* x0, const int* iter, cudaStream_t s) const;
+    // sum over the hop entries of the row of src, with K = uint32_t up to 32
+    // sites (reps32 set) and uint64_t beyond
+    template <class K, class V>
+    __device__ __forceinline__ V hop_sum(K src, const V* __restrict__ xsv) const {
+        V acc = Sc<V>::zero();
+        for (int base = 0; base < n_hops; base += 64) {
+            const int nb = min(64, n_hops - base);
+            uint64_t live = 0;
+            for (int b = 0; b < nb; ++b) {
+                const int odd = sizeof(K) == 4 ? __popc((uint32_t)src & s_pair32[base + b])
+                                               : __popcll((uint64_t)src & s_hops[base + b].pair);
+                live |= (uint64_t)(odd & 1) << b;
+            }
+            while (live) {
+                const int b = base + __ffsll((long long)live) - 1;
+                live &= live - 1;
+                const K pair = sizeof(K) == 4 ? (K)s_pair32[b] : (K)s_hops[b].pair;
+                const K t = src ^ pair;
+                const double2 cf = s_hop_c[2 * b + ((src & pair & (K(0) - pair)) ? 1 : 0)];
+                if (hop_one_way && cf.x == 0.0 && cf.y == 0.0) continue;  // no term in this direction
+                int e, found;
+                int64_t c;
+                if constexpr (sizeof(K) == 4) {
+                    const uint32_t rr = rg.g.full_rot ? chain_orbit_min(rg.g, gs, t, &e)
+                                                      : (uint32_t)orbit_min(rg.g, gs, t, &e);
+                    uint32_t c32;
+                    found = look.find32(rg, rr, &c32);
+                    c = c32;
+                } else {
+                    const uint64_t rr = orbit_min(rg.g, gs, t, &e);
+                    double f;
+                    found = look.find(rg, rr, &c, &f);
+                }
+                if (found <= 0) {
+                    if (found < 0) *rg.err = 2;
+                    continue;
+                }
+                const double2 ch = rg.g.chars[e];
+                const double2 v = make_double2(cf.x * ch.x + cf.y * ch.y, cf.y * ch.x - cf.x * ch.y);
+                acc = Sc<V>::fma(Sc<V>::from(v), __ldg(xsv + c), acc);
+            }
+        }
+        return acc;
+    }
     template <class V>
     __device__ __forceinline__ V row(int64_t r, const V* __restrict__ x, V& xr) const {
-        int64_t o = rg.orbit_of_row[r];
-        uint64_t src = apply_elem(rg.g, gs, 0, rg.rt.reps[o]);
-        double ns = rg.norms[o];
+        const uint64_t rep = look.reps32 ? (uint64_t)look.reps32[r] : look.reps64[r];
+        const uint64_t src = apply_elem(rg.g, gs, 0, rep);
+        const V* __restrict__ xsv = reinterpret_cast<const V*>(xs);
         xr = x[r];
-        V acc = Sc<V>::zero();
-        double2 d = gen_row(rg, gs, ts, src, ns, [&](int64_t ot, double2 v) {
-            int64_t c = rg.row_of_orbit[ot];
-            acc = Sc<V>::fma(Sc<V>::from(v), __ldg(x + c), acc);
-        });
+        V acc;
+        double2 d;
+        if (n_hops) {
+            acc = look.reps32 ? hop_sum<uint32_t, V>((uint32_t)src, xsv) : hop_sum<uint64_t, V>(src, xsv);
+            d = cplx ? reinterpret_cast<const double2*>(diag)[r]
+                     : make_double2(reinterpret_cast<const double*>(diag)[r], 0.0);
+        } else {
+            acc = Sc<V>::zero();
+            d = gen_row_look(rg, gs, ts, 0, ts.n_terms, src, look, [&](int64_t c, double2 v) {
+                acc = Sc<V>::fma(Sc<V>::from(v), __ldg(xsv + c), acc);
+            });
+        }
+        acc = Sc<V>::scale(acc, 1.0 / nrow[r]);
         acc = Sc<V>::fma(Sc<V>::from(d), xr, acc);
         return acc;
     }
 };
+
+// Minimum resident blocks of 256 threads a product kernel over Op is compiled
+// for: the matrix-free operator is issue- and latency-bound and runs best at
+// five (at most 48 registers a thread).
+template <class Op> struct OpMinBlocks { static constexpr int value = 1; };
+template <class M> struct OpMinBlocks<MfOp<M>> { static constexpr int value = 5; };
+
+// xs = n(c) x_c for the matrix-free operator, where x = x0, or with iter the
+// half of the Lanczos work buffer x0 that step *iter reads.
+template <class V>
+__global__ void __launch_bounds__(256) k_mf_scale(int64_t n, const double* __restrict__ nrow,
+                                                  const V* __restrict__ x0, const int* __restrict__ iter,
+                                                  V* __restrict__ xs) {
+    const V* x = x0 + (iter ? (int64_t)((*iter) & 1) * n : 0);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        xs[r] = Sc<V>::scale(x[r], nrow[r]);
+}
+
+template <class M>
+template <class V>
+void MfOp<M>::pre(const V* x0, const int* iter, cudaStream_t s) const {
+    k_mf_scale<V><<<grid_for(n, 256), 256, 0, s>>>(n, nrow, x0, iter, reinterpret_cast<V*>(xs));
+}
 
 }  // namespace qmb
 
@@ -356,6 +601,21 @@ struct qmb_ham_s {
     qmb::DevBuf<uint16_t> t_ops;
     qmb::DevBuf<double2> t_scalar;
     qmb::DevBuf<int> err;
+    // hop form of the terms (n_hops > 0), for the matrix-free operator
+    int n_hops = 0;
+    int hop_one_way = 0;
+    qmb::DevBuf<qmb::Hop> hops;
+    qmb::DevBuf<double2> hop_c;
+    // matrix-free lookup over the active orbits (mf_tables(), on first use)
+    bool mf_ready = false;
+    int mf_shift = 0;
+    uint64_t mf_nb = 0;
+    qmb::DevBuf<uint32_t> mf_reps32;   // [n] active representatives, L <= 32
+    qmb::DevBuf<uint64_t> mf_reps64;   // [n] L > 32 with null orbits (else the sector's table)
+    qmb::DevBuf<uint32_t> mf_bucket;   // [mf_nb + 1]
+    qmb::DevBuf<double> mf_norm;       // [n] norm of each row's orbit
+    qmb::DevBuf<unsigned char> mf_diag;  // [n] diagonal with a hop table (double2 if complex)
+    qmb::DevBuf<unsigned char> mf_xs;  // [n] n(c) x_c in the product's vector type
     // ground state kept by qmb_lanczos
     qmb::DevBuf<unsigned char> psi;
     int64_t psi_n = 0;
@@ -407,16 +667,37 @@ struct qmb_ham_s {
         op.sdict = nullptr;
         return op;
     }
+    // the matrix-free operator (mf_tables() must have run)
     template <class M> qmb::MfOp<M> mf() const {
         qmb::MfOp<M> op;
         op.n = n;
         op.rg = row_gen();
+        op.look.reps32 = mf_reps32.p;
+        op.look.reps64 = mf_reps32.p ? nullptr : (mf_reps64.p ? mf_reps64.p : sector->reps.p);
+        op.look.bucket = mf_bucket.p;
+        op.look.shift = mf_shift;
+        op.look.n_b = mf_nb;
+        op.look.n = n;
+        op.look.all_active = sector->n_active == sector->R ? 1 : 0;
+        op.nrow = mf_norm.p;
+        op.xs = mf_xs.p;
+        op.n_hops = n_hops;
+        op.hop_one_way = hop_one_way;
+        op.hops = hops.p;
+        op.hop_c = hop_c.p;
+        op.diag = mf_diag.p;
+        op.cplx = cplx ? 1 : 0;
+        op.s_hops = nullptr;
+        op.s_pair32 = nullptr;
+        op.s_hop_c = nullptr;
         op.gbytes = qmb::group_smem_bytes(op.rg.g);
         return op;
     }
 };
 
 namespace qmb {
+// Builds the matrix-free operator's tables on the handle (once).
+void mf_tables(qmb_ham_s* h);
 // Upload operator tables (validated) into the handle's term buffers.
 void upload_terms(qmb_ham_s* h, const qmb_terms* t, int L);
 int grid_for(int64_t n, int block);

@@ -99,7 +99,7 @@ __global__ void k_lz_start(int64_t n, int mode, uint64_t seed, const P* __restri
 // K1: y = H w_j / beta_j - beta_j v_{j-1}; v_j = w_j / beta_j; alpha_j = Re <v_j, y>.
 // Optionally psi += c_j v_j (eigenvector regeneration).
 template <class Op, class V, class P>
-__global__ void __launch_bounds__(kLzBlock) k_lz_hv(Op op, V* __restrict__ wbuf, V* __restrict__ vring,
+__global__ void __launch_bounds__(kLzBlock, OpMinBlocks<Op>::value) k_lz_hv(Op op, V* __restrict__ wbuf, V* __restrict__ vring,
                                                     int K, LzDev d, const double* __restrict__ ritz,
                                                     P* __restrict__ psi) {
     extern __shared__ __align__(16) unsigned char smem_lz[];
@@ -359,7 +359,7 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
     if (po.reorth) set_group_smem_attr((const void*)k_reorth_update<V>, ro_smem);
 
     auto step = [&](cudaStream_t ss) {
-        op.pre((const V*)wbuf.p, st.d.iter, ss);  // earlier column-block passes, if any
+        op.pre((const V*)wbuf.p, st.d.iter, ss);  // column-block passes or the matrix-free scaling, if any
         k_lz_hv<Op, V, P><<<nb, kLzBlock, op_smem, ss>>>(op, wbuf.p, vring.p, K, st.d, nullptr,
                                                          (P*)nullptr);
         k_lz_update<V><<<nb, kLzBlock, 0, ss>>>(n, wbuf.p, vring.p, K, st.d, po.reorth ? 0 : 1);
@@ -713,6 +713,8 @@ extern "C" qmb_status qmb_lanczos(qmb_ham h, const qmb_lanczos_opts* opts, qmb_l
         if (!mf) {
             QMB_REQUIRE(!need64 || h->val64.p, QMB_ERR_INVALID, "handle holds no FP64 values");
             QMB_REQUIRE(!need32 || h->val32.p, QMB_ERR_INVALID, "handle holds no FP32 values");
+        } else {
+            mf_tables(h);
         }
         if (h->cplx) {
             if (mf) {

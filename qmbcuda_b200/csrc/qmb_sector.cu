@@ -290,6 +290,14 @@ void sector_setup(qmb_sector_s* s, const qmb_sector_desc* d) {
         }
     s->structured = structured ? 1 : 0;
     s->n_chunks = (L + 3) / 4;
+    // all L rotations of a chain of at most 32 sites, element 0 the identity
+    s->full_rot = 0;
+    if (structured && s->W == L && G == L && L <= 32 && rots[0].ri == 0) {
+        std::vector<int> seen(L, 0);
+        bool distinct = true;
+        for (int g = 0; g < G; ++g) distinct = distinct && !seen[rots[g].ri]++;
+        s->full_rot = distinct ? 1 : 0;
+    }
     if (structured) {
         s->rot.alloc(G);
         s->rot.upload(rots.data(), G);

@@ -13,6 +13,7 @@ struct qmb_sector_s {
 
     // group on device
     int structured = 0, W = 0, n_chunks = 0;
+    int full_rot = 0;  // a chain group of all L <= 32 rotations, element 0 the identity
     qmb::DevBuf<qmb::ElemRot> rot;
     qmb::DevBuf<uint64_t> tables;
 
@@ -41,6 +42,7 @@ struct qmb_sector_s {
         g.structured = structured;
         g.W = W;
         g.n_chunks = n_chunks;
+        g.full_rot = full_rot;
         g.mask = (L == 64) ? ~0ull : ((1ull << L) - 1);
         g.rot = rot.p;
         g.tables = tables.p;

@@ -147,6 +147,51 @@ def test_hv_stored_and_matrix_free(case):
     np.testing.assert_allclose(yd.cpu().numpy(), y_o, rtol=0, atol=1e-12 * np.abs(y_o).max())
 
 
+@pytest.mark.parametrize("L,k,flip,a", [(12, 6, False, 0), (12, 6, False, 1), (16, 8, True, 3),
+                                         (32, 4, False, 0), (32, 4, False, 1), (36, 3, False, 0),
+                                         (36, 3, False, 1), (34, 4, False, 11)],
+                         ids=lambda v: str(v))
+def test_matrix_free_active_lookup(L, k, flip, a):
+    """The matrix-free operator's row lookup over the active orbits: 32-bit
+    representatives up to L = 32 (the run-candidate orbit minimum of full
+    rotation groups, funnel shifts at L = 32), 64-bit beyond; the sector's
+    tables when every orbit is active, its own bucket table when some orbits
+    are null.  FP64 and FP32 products against the oracle's matrix, and a
+    matrix-free FP64 solve against the stored one."""
+    import torch
+    perm, ch = q.translation_group(L)
+    chars = np.block([[ch, ch], [ch, -ch]]) if flip else ch
+    terms = q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), [1.0] * L + [0.3] * L, 0.7)
+    sec_o = O.build_sector(oracle_group(perm, chars, flip), k)
+    s = q.Sector(L, k, perm, spin_flip=flip).set_irrep(chars[a])
+    act = O.active_rows(sec_o, a)
+    assert (len(act) < sec_o.R) == (a != 0), "the cases cover both table forms"
+    h = q.Hamiltonian(s, terms)
+    W = 4 * L + 1
+    rc, ind_o, val_o, tr_o = O.ell_terms(sec_o, oracle_terms(terms), a, W)
+    assert rc >= 0
+    A = O.ell_to_csr(ind_o, val_o, tr_o, act)
+    n = A.shape[0]
+    assert h.info.n_rows == n
+    rng = np.random.default_rng(L + a)
+    x = rng.standard_normal(n) + (1j * rng.standard_normal(n) if h.info.is_complex else 0)
+    y_o = A @ x
+    for prec, tol in ((q._capi.PREC_FP64, 1e-12), (q._capi.PREC_FP32, 2e-6)):
+        if prec == q._capi.PREC_FP64:
+            dt = torch.complex128 if h.info.is_complex else torch.float64
+        else:
+            dt = torch.complex64 if h.info.is_complex else torch.float32
+        xd = torch.tensor(x, dtype=dt, device="cuda")
+        yd = torch.zeros_like(xd)
+        h.hv_dev(xd.data_ptr(), yd.data_ptr(), prec, matrix_free=True)
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(yd.cpu().numpy(), y_o, rtol=0, atol=tol * np.abs(y_o).max())
+    A64 = q._capi
+    r_st = h.lanczos(mode=A64.MODE_FP64, tol=1e-12)
+    r_mf = h.lanczos(mode=A64.MODE_FP64, tol=1e-12, hv=A64.HV_MATRIX_FREE)
+    assert abs(r_mf.E0 - r_st.E0) <= 1e-10 * abs(r_st.E0)
+
+
 @pytest.mark.parametrize("a", [0, 3])
 def test_column_blocked_product_and_solve(a, monkeypatch):
     """The column-blocked coded FP32 layout (built for vectors larger than L2;

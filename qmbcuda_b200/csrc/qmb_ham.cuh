@@ -616,6 +616,11 @@ struct qmb_ham_s {
     qmb::DevBuf<double> mf_norm;       // [n] norm of each row's orbit
     qmb::DevBuf<unsigned char> mf_diag;  // [n] diagonal with a hop table (double2 if complex)
     qmb::DevBuf<unsigned char> mf_xs;  // [n] n(c) x_c in the product's vector type
+    // Lanczos buffers kept between qmb_lanczos calls (one call at a time on
+    // a handle): the stored basis ring, the two work vectors, and the ring
+    // slots the last solve used
+    qmb::DevBuf<unsigned char> lz_ring, lz_wbuf;
+    int lz_ring_hint = 0;
     // ground state kept by qmb_lanczos
     qmb::DevBuf<unsigned char> psi;
     int64_t psi_n = 0;

@@ -155,30 +155,57 @@ __global__ void __launch_bounds__(kLzBlock) k_lz_update(int64_t n, V* __restrict
     }
 }
 
-// Reorthogonalisation, pass 1: coefs[i] = <v_i, w_{j+1}> for i <= j.
+// Reorthogonalisation, pass 1: coefs[i] = <v_i, w_{j+1}> for i <= j, eight
+// basis vectors a sweep over the rows (w is read once per eight).
+constexpr int kDotChunk = 8;
 template <class V>
 __global__ void __launch_bounds__(kLzBlock) k_reorth_dots(int64_t n, const V* __restrict__ wbuf,
                                                           const V* __restrict__ vring, LzDev d) {
-    __shared__ double red[32];
+    __shared__ double red[2 * kDotChunk * (kLzBlock / 32)];
     __shared__ bool last;
     const int j = *d.iter;
     const V* Y = wbuf + (int64_t)((j + 1) & 1) * n;
     const int nb = gridDim.x;
-    for (int i = 0; i <= j; ++i) {
-        const V* Vi = vring + (int64_t)i * n;
-        double re = 0.0, im = 0.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+    for (int i0 = 0; i0 <= j; i0 += kDotChunk) {
+        const int cnt = min(kDotChunk, j + 1 - i0);
+        double re[kDotChunk], im[kDotChunk];
+#pragma unroll
+        for (int k = 0; k < kDotChunk; ++k) re[k] = im[k] = 0.0;
         for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
              r += (int64_t)gridDim.x * blockDim.x) {
-            V v = Vi[r], y = Y[r];
-            re += Sc<V>::re_conj_mul(v, y);
-            if constexpr (Sc<V>::cplx) im += Sc<V>::im_conj_mul(v, y);
+            const V y = Y[r];
+#pragma unroll
+            for (int k = 0; k < kDotChunk; ++k)
+                if (k < cnt) {
+                    const V v = vring[(int64_t)(i0 + k) * n + r];
+                    re[k] += Sc<V>::re_conj_mul(v, y);
+                    if constexpr (Sc<V>::cplx) im[k] += Sc<V>::im_conj_mul(v, y);
+                }
         }
-        double bre = block_sum(re, red);
-        double bim = Sc<V>::cplx ? block_sum(im, red) : 0.0;
-        if (threadIdx.x == 0) {
-            d.cpart[2 * ((int64_t)i * nb + blockIdx.x)] = bre;
-            d.cpart[2 * ((int64_t)i * nb + blockIdx.x) + 1] = bim;
+#pragma unroll
+        for (int k = 0; k < kDotChunk; ++k)
+            for (int o = 16; o > 0; o >>= 1) {
+                re[k] += __shfl_xor_sync(0xffffffffu, re[k], o);
+                im[k] += __shfl_xor_sync(0xffffffffu, im[k], o);
+            }
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < kDotChunk; ++k) {
+                red[2 * (warp * kDotChunk + k)] = re[k];
+                red[2 * (warp * kDotChunk + k) + 1] = im[k];
+            }
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+            double bre = 0.0, bim = 0.0;
+            for (int w = 0; w < n_warps; ++w) {
+                bre += red[2 * (w * kDotChunk + threadIdx.x)];
+                bim += red[2 * (w * kDotChunk + threadIdx.x) + 1];
+            }
+            d.cpart[2 * ((int64_t)(i0 + threadIdx.x) * nb + blockIdx.x)] = bre;
+            d.cpart[2 * ((int64_t)(i0 + threadIdx.x) * nb + blockIdx.x) + 1] = bim;
         }
+        __syncthreads();
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -188,13 +215,18 @@ __global__ void __launch_bounds__(kLzBlock) k_reorth_dots(int64_t n, const V* __
     __syncthreads();
     if (!last) return;
     __threadfence();
-    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+    // the last block: one warp per coefficient sums the blocks' partials
+    for (int i = warp; i <= j; i += n_warps) {
         double re = 0.0, im = 0.0;
-        for (int b = 0; b < nb; ++b) {
+        for (int b = lane; b < nb; b += 32) {
             re += __ldcg(d.cpart + 2 * ((int64_t)i * nb + b));
             im += __ldcg(d.cpart + 2 * ((int64_t)i * nb + b) + 1);
         }
-        d.coefs[i] = make_double2(re, im);
+        for (int o = 16; o > 0; o >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (lane == 0) d.coefs[i] = make_double2(re, im);
     }
     __syncthreads();
     if (threadIdx.x == 0) *d.counter = 0;
@@ -318,7 +350,26 @@ struct PhaseOut {
     int n_hv = 0;
 };
 
+// A typed view of a byte buffer that only grows: alloc(count) keeps the
+// memory when it is large enough, so the handle's Lanczos buffers persist
+// between solves instead of being allocated and freed (tens of ms for a
+// stored basis of several GB) every time.
+template <class V>
+struct GrowBuf {
+    DevBuf<unsigned char>* bytes;
+    V* p = nullptr;
+    explicit GrowBuf(DevBuf<unsigned char>* b) : bytes(b) {}
+    void alloc(size_t count) {
+        if (bytes->n < count * sizeof(V)) {
+            bytes->release();
+            bytes->alloc(count * sizeof(V));
+        }
+        p = reinterpret_cast<V*>(bytes->p);
+    }
+};
+
 struct PhaseOpts {
+    int* ring_hint = nullptr;  // in/out: stored-basis slots to start with
     int max_iter = 200;
     int min_iter = 1;
     double tol = 1e-12;       // <= 0: run exactly max_iter steps
@@ -334,15 +385,21 @@ struct PhaseOpts {
 
 // Runs one Lanczos phase for operator op with vectors of type V.
 // start_mode 0/1: generated from seed, 2: copied from `from` (type P).
+// With `store` the basis is kept for the Ritz vector (and any
+// reorthogonalisation): the ring starts with the slots the hint asks for
+// (the previous phase's steps plus a check block) and doubles, its filled
+// slots copied over, before a block of steps would wrap it.
 template <class Op, class V, class P>
 PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_mode,
-                   uint64_t seed, const P* from, bool store, DevBuf<V>& vring, int& K,
-                   DevBuf<V>& wbuf, LzState& st, cudaStream_t s) {
+                   uint64_t seed, const P* from, bool store, GrowBuf<V>& vring, int& K,
+                   GrowBuf<V>& wbuf, LzState& st, cudaStream_t s) {
     const int64_t n = op.n;
     PhaseOut out;
     const double gap_cap = restart_gap_cap();
     int cap = std::max(1, po.max_iter);
-    K = store ? cap + 1 : 2;
+    const int K_full = store ? cap + 1 : 2;
+    const int hint = po.ring_hint ? *po.ring_hint : 0;
+    K = store ? std::min(K_full, std::max({hint, 2 + std::max(1, po.check_every), 32})) : 2;
     vring.alloc((size_t)K * n);
     wbuf.alloc(2 * (size_t)n);
     st.init(cap, lz_blocks(), po.reorth > 0);
@@ -372,7 +429,12 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
 
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
-    if (po.use_graph) {
+    auto capture = [&]() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        if (!po.use_graph) return;
         QMB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         step(s);
         cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -381,8 +443,9 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
             cudaGetLastError();
             exec = nullptr;
         }
-    }
-    check_launch("lanczos step capture");
+        check_launch("lanczos step capture");
+    };
+    capture();
 
     std::vector<double> ha(cap + 1), hb(cap + 2);
     int done = 0;
@@ -391,6 +454,20 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
     const int every = std::max(1, po.check_every);
     while (done < cap) {
         int todo = std::min(every, cap - done);
+        if (store && done + todo > K) {
+            // steps done .. done+todo-1 write slots j: grow the ring first
+            const int K2 = std::min(K_full, std::max(2 * K, done + todo));
+            DevBuf<unsigned char> grown;
+            grown.alloc((size_t)K2 * n * sizeof(V));
+            QMB_CUDA_TRY(cudaMemcpyAsync(grown.p, vring.p, (size_t)done * n * sizeof(V),
+                                         cudaMemcpyDeviceToDevice, s));
+            QMB_CUDA_TRY(cudaStreamSynchronize(s));
+            std::swap(vring.bytes->p, grown.p);
+            std::swap(vring.bytes->n, grown.n);
+            vring.p = reinterpret_cast<V*>(vring.bytes->p);
+            K = K2;
+            capture();
+        }
         for (int t = 0; t < todo; ++t) {
             if (exec) QMB_CUDA_TRY(cudaGraphLaunch(exec, s));
             else step(s);
@@ -475,6 +552,7 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
         have_prev = true;
     }
     if (po.tol <= 0) out.converged = true;
+    if (store && po.ring_hint) *po.ring_hint = std::max(*po.ring_hint, out.m + 1 + every);
     out.a.assign(ha.begin(), ha.begin() + out.m);
     out.e.assign(hb.begin() + 1, hb.begin() + out.m);
     if (exec) cudaGraphExecDestroy(exec);
@@ -483,9 +561,9 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
 }
 
 // psi = Ritz vector of a finished phase (stored basis, else regeneration).
-template <class Op, class V, class P>
+template <class Op, class V, class P, class Buf>
 void ritz_vector(const Op& op, size_t op_smem, const PhaseOut& ph, int start_mode, uint64_t seed,
-                 const P* from, bool stored, DevBuf<V>& vring, int K, DevBuf<V>& wbuf,
+                 const P* from, bool stored, Buf& vring, int K, Buf& wbuf,
                  LzState& st, P* psi, int& n_hv, cudaStream_t s, bool for_restart = false) {
     const int64_t n = op.n;
     DevBuf<double> ritz(ph.m);
@@ -567,10 +645,11 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     PhaseOut last;
 
     // full FP64 solve from the seeded start vector
+    po.ring_hint = &h->lz_ring_hint;
     auto fp64_solve = [&]() {
         bool store = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap + 3) * n);
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
-        DevBuf<V64> vr, wb;
+        GrowBuf<V64> vr(&h->lz_ring), wb(&h->lz_wbuf);
         int K;
         last = run_phase<Op64, V64, V64>(op64, sm64, po, o.start, o.seed, nullptr, store, vr, K, wb, st, s);
         n_hv += last.n_hv;
@@ -602,7 +681,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
         PhaseOut ph1;
         {
-            DevBuf<V32> vr, wb;
+            GrowBuf<V32> vr(&h->lz_ring), wb(&h->lz_wbuf);
             int K;
             ph1 = run_phase<Op32, V32, V64>(op32, sm32, p1, o.start, o.seed, nullptr, store, vr, K, wb, st, s);
             n_hv += ph1.n_hv;
@@ -626,7 +705,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
             bool store2 = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap2 + 3) * n);
             DevBuf<V64> start(n);
             QMB_CUDA_TRY(cudaMemcpyAsync(start.p, psi.p, sizeof(V64) * n, cudaMemcpyDeviceToDevice, s));
-            DevBuf<V64> vr, wb;
+            GrowBuf<V64> vr(&h->lz_ring), wb(&h->lz_wbuf);
             int K;
             PhaseOut ph2 = run_phase<Op64, V64, V64>(op64, sm64, p2, 2, 0, start.p, store2, vr, K,
                                                      wb, st, s);

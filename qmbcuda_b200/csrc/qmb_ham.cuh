@@ -393,25 +393,40 @@ struct ActiveLookup {
         if (all_active) return -1;
         return find_rep(rg.rt, r) < 0 ? -1 : 0;  // a null orbit, or outside the sector
     }
-    // find() for L <= 32 (reps32 set), in 32-bit arithmetic
-    __device__ __forceinline__ int find32(const RowGen& rg, uint32_t r, uint32_t* idx) const {
-        const uint32_t b = r >> shift;
-        uint32_t lo = 0, hi = 0;
-        if (b < (uint32_t)n_b) {
-            lo = bucket[b];
-            hi = bucket[b + 1];
+    // find() of two representatives at once for L <= 32 (reps32 set), in
+    // 32-bit arithmetic: the two searches run in
+    // lockstep, so each step has two independent loads in flight
+    __device__ __forceinline__ void find32x2(const RowGen& rg, uint32_t r1, uint32_t r2, uint32_t* i1,
+                                             uint32_t* i2, int* f1, int* f2) const {
+        const uint32_t b1 = r1 >> shift, b2 = r2 >> shift;
+        uint32_t lo1 = 0, hi1 = 0, lo2 = 0, hi2 = 0;
+        if (b1 < (uint32_t)n_b) {
+            lo1 = bucket[b1];
+            hi1 = bucket[b1 + 1];
         }
-        while (lo < hi) {
-            const uint32_t mid = lo + ((hi - lo) >> 1);
-            if (__ldg(reps32 + mid) < r) lo = mid + 1;
-            else hi = mid;
+        if (b2 < (uint32_t)n_b) {
+            lo2 = bucket[b2];
+            hi2 = bucket[b2 + 1];
         }
-        if (lo < (uint32_t)n && __ldg(reps32 + lo) == r) {
-            *idx = lo;
-            return 1;
+        while (lo1 < hi1 || lo2 < hi2) {
+            const bool a1 = lo1 < hi1, a2 = lo2 < hi2;
+            const uint32_t m1 = lo1 + ((hi1 - lo1) >> 1), m2 = lo2 + ((hi2 - lo2) >> 1);
+            const uint32_t v1 = a1 ? __ldg(reps32 + m1) : 0u, v2 = a2 ? __ldg(reps32 + m2) : 0u;
+            if (a1) {
+                if (v1 < r1) lo1 = m1 + 1;
+                else hi1 = m1;
+            }
+            if (a2) {
+                if (v2 < r2) lo2 = m2 + 1;
+                else hi2 = m2;
+            }
         }
-        if (all_active) return -1;
-        return find_rep(rg.rt, r) < 0 ? -1 : 0;
+        const uint32_t nn = (uint32_t)n;
+        const uint32_t w1 = lo1 < nn ? __ldg(reps32 + lo1) : ~r1, w2 = lo2 < nn ? __ldg(reps32 + lo2) : ~r2;
+        *i1 = lo1;
+        *i2 = lo2;
+        *f1 = w1 == r1 ? 1 : (all_active ? -1 : (find_rep(rg.rt, r1) < 0 ? -1 : 0));
+        *f2 = w2 == r2 ? 1 : (all_active ? -1 : (find_rep(rg.rt, r2) < 0 ? -1 : 0));
     }
 };
 
@@ -482,39 +497,25 @@ struct MfOp {
     }
     template <class V>
     void pre(const V* x0, const int* iter, cudaStream_t s) const;
-    // sum over the hop entries of the row of src, with K = uint32_t up to 32
-    // sites (reps32 set) and uint64_t beyond
-    template <class K, class V>
-    __device__ __forceinline__ V hop_sum(K src, const V* __restrict__ xsv) const {
+    // sum over the hop entries of the row of src (strings beyond 32 sites)
+    template <class V>
+    __device__ __forceinline__ V hop_sum64(uint64_t src, const V* __restrict__ xsv) const {
         V acc = Sc<V>::zero();
         for (int base = 0; base < n_hops; base += 64) {
             const int nb = min(64, n_hops - base);
             uint64_t live = 0;
-            for (int b = 0; b < nb; ++b) {
-                const int odd = sizeof(K) == 4 ? __popc((uint32_t)src & s_pair32[base + b])
-                                               : __popcll((uint64_t)src & s_hops[base + b].pair);
-                live |= (uint64_t)(odd & 1) << b;
-            }
+            for (int b = 0; b < nb; ++b) live |= (uint64_t)(__popcll(src & s_hops[base + b].pair) & 1) << b;
             while (live) {
                 const int b = base + __ffsll((long long)live) - 1;
                 live &= live - 1;
-                const K pair = sizeof(K) == 4 ? (K)s_pair32[b] : (K)s_hops[b].pair;
-                const K t = src ^ pair;
-                const double2 cf = s_hop_c[2 * b + ((src & pair & (K(0) - pair)) ? 1 : 0)];
+                const uint64_t pair = s_hops[b].pair;
+                const double2 cf = s_hop_c[2 * b + ((src & pair & (0ull - pair)) ? 1 : 0)];
                 if (hop_one_way && cf.x == 0.0 && cf.y == 0.0) continue;  // no term in this direction
-                int e, found;
+                int e;
+                const uint64_t rr = orbit_min(rg.g, gs, src ^ pair, &e);
                 int64_t c;
-                if constexpr (sizeof(K) == 4) {
-                    const uint32_t rr = rg.g.full_rot ? chain_orbit_min(rg.g, gs, t, &e)
-                                                      : (uint32_t)orbit_min(rg.g, gs, t, &e);
-                    uint32_t c32;
-                    found = look.find32(rg, rr, &c32);
-                    c = c32;
-                } else {
-                    const uint64_t rr = orbit_min(rg.g, gs, t, &e);
-                    double f;
-                    found = look.find(rg, rr, &c, &f);
-                }
+                double f;
+                const int found = look.find(rg, rr, &c, &f);
                 if (found <= 0) {
                     if (found < 0) *rg.err = 2;
                     continue;
@@ -522,6 +523,56 @@ struct MfOp {
                 const double2 ch = rg.g.chars[e];
                 const double2 v = make_double2(cf.x * ch.x + cf.y * ch.y, cf.y * ch.x - cf.x * ch.y);
                 acc = Sc<V>::fma(Sc<V>::from(v), __ldg(xsv + c), acc);
+            }
+        }
+        return acc;
+    }
+    // the same up to 32 sites (reps32 set) in 32-bit arithmetic, taking the
+    // row's entries two at a time: both orbit minima, then both lookups in
+    // lockstep, then both gathers
+    template <class V>
+    __device__ __forceinline__ V hop_sum32x2(uint32_t src, const V* __restrict__ xsv) const {
+        V acc = Sc<V>::zero();
+        for (int base = 0; base < n_hops; base += 64) {
+            const int nb = min(64, n_hops - base);
+            uint64_t live = 0;
+            for (int b = 0; b < nb; ++b) live |= (uint64_t)(__popc(src & s_pair32[base + b]) & 1) << b;
+            while (live) {
+                const int b1 = base + __ffsll((long long)live) - 1;
+                live &= live - 1;
+                const bool two = live != 0;
+                const int b2 = two ? base + __ffsll((long long)live) - 1 : b1;
+                live &= live - (two ? 1 : 0);
+                const uint32_t p1 = s_pair32[b1], p2 = s_pair32[b2];
+                const double2 cf1 = s_hop_c[2 * b1 + ((src & p1 & (0u - p1)) ? 1 : 0)];
+                const double2 cf2 = s_hop_c[2 * b2 + ((src & p2 & (0u - p2)) ? 1 : 0)];
+                int e1, e2;
+                const uint32_t t1 = src ^ p1, t2 = src ^ p2;
+                const uint32_t r1 = rg.g.full_rot ? chain_orbit_min(rg.g, gs, t1, &e1)
+                                                  : (uint32_t)orbit_min(rg.g, gs, t1, &e1);
+                const uint32_t r2 = rg.g.full_rot ? chain_orbit_min(rg.g, gs, t2, &e2)
+                                                  : (uint32_t)orbit_min(rg.g, gs, t2, &e2);
+                uint32_t c1, c2;
+                int f1, f2;
+                look.find32x2(rg, r1, r2, &c1, &c2, &f1, &f2);
+                // a direction without a term (one-way hops) contributes nothing
+                const bool z1 = hop_one_way && cf1.x == 0.0 && cf1.y == 0.0;
+                const bool z2 = !two || (hop_one_way && cf2.x == 0.0 && cf2.y == 0.0);
+                if (!z1 && f1 < 0) *rg.err = 2;
+                if (!z2 && f2 < 0) *rg.err = 2;
+                const bool u1 = !z1 && f1 > 0, u2 = !z2 && f2 > 0;
+                const V x1 = u1 ? __ldg(xsv + c1) : Sc<V>::zero();
+                const V x2 = u2 ? __ldg(xsv + c2) : Sc<V>::zero();
+                if (u1) {
+                    const double2 ch = rg.g.chars[e1];
+                    acc = Sc<V>::fma(Sc<V>::from(make_double2(cf1.x * ch.x + cf1.y * ch.y, cf1.y * ch.x - cf1.x * ch.y)),
+                                     x1, acc);
+                }
+                if (u2) {
+                    const double2 ch = rg.g.chars[e2];
+                    acc = Sc<V>::fma(Sc<V>::from(make_double2(cf2.x * ch.x + cf2.y * ch.y, cf2.y * ch.x - cf2.x * ch.y)),
+                                     x2, acc);
+                }
             }
         }
         return acc;
@@ -535,7 +586,7 @@ struct MfOp {
         V acc;
         double2 d;
         if (n_hops) {
-            acc = look.reps32 ? hop_sum<uint32_t, V>((uint32_t)src, xsv) : hop_sum<uint64_t, V>(src, xsv);
+            acc = look.reps32 ? hop_sum32x2<V>((uint32_t)src, xsv) : hop_sum64<V>(src, xsv);
             d = cplx ? reinterpret_cast<const double2*>(diag)[r]
                      : make_double2(reinterpret_cast<const double*>(diag)[r], 0.0);
         } else {

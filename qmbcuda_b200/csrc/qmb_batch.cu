@@ -1848,12 +1848,29 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
     // Ritz vectors (FP64) for the next phase or the caller
     if (psi_out) {
         Buf<double> xs = ws_take<double>((size_t)(cap + 1) * n_prob);
+        cudaEvent_t te[3] = {nullptr, nullptr, nullptr};
+        if (trace_on())
+            for (auto& e : te) {
+                QMB_CUDA_TRY(cudaEventCreate(&e));
+            }
+        if (te[0]) QMB_CUDA_TRY(cudaEventRecord(te[0], st));
         g_kernels += 1;
         k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p, gap_out);
+        if (te[1]) QMB_CUDA_TRY(cudaEventRecord(te[1], st));
         if (K > 2 && done < K) {
             g_kernels += 1;
             k_bpsi<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, vring.p, K, msteps.p, ritz.p, n_prob,
                                                           psi_out);
+            if (te[2]) {
+                QMB_CUDA_TRY(cudaEventRecord(te[2], st));
+                QMB_CUDA_TRY(cudaEventSynchronize(te[2]));
+                float a_ms = 0, b_ms = 0;
+                cudaEventElapsedTime(&a_ms, te[0], te[1]);
+                cudaEventElapsedTime(&b_ms, te[1], te[2]);
+                std::fprintf(stderr, "[qmb batch] ritz: k_britz %.2f ms, k_bpsi %.2f ms (device), %.2f ms to here\n",
+                             a_ms, b_ms,
+                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count());
+            }
         } else {
             QMB_CUDA_TRY(cudaMemsetAsync(psi_out, 0, (Sc<V>::cplx ? 16 : 8) * tot, st));
             std::vector<int> all(k.n_sectors, 1);
@@ -1875,6 +1892,8 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             }
         }
         check_launch("batch ritz");
+        for (auto& e : te)
+            if (e) cudaEventDestroy(e);
     }
     out.theta.resize(n_prob);
     out.msteps.resize(n_prob);
@@ -2283,6 +2302,24 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                 ph = p1;
                 it_tot = std::max(it_tot, p1.steps);
                 if (o.mode == QMB_MODE_MIXED) {
+                    if (trace_on()) {
+                        std::fprintf(stderr, "[qmb batch] fp32 phase returned at %.2f ms\n", solve_ms());
+                        // steps each problem needed, and the last step of each sector
+                        int hist[8] = {0};
+                        std::string smax;
+                        for (int s = 0; s < k.n_sectors; ++s) {
+                            int mx = 0;
+                            for (int set = 0; set < b->n_sets; ++set) {
+                                const int m = p1.msteps[(size_t)s * b->nsp + set];
+                                mx = std::max(mx, m);
+                                hist[std::min(7, m / 20)]++;
+                            }
+                            smax += " " + std::to_string(mx);
+                        }
+                        std::fprintf(stderr, "[qmb batch] fp32 steps per problem 0-19..140+: %d %d %d %d %d %d %d %d; "
+                                     "per sector max:%s\n", hist[0], hist[1], hist[2], hist[3], hist[4], hist[5],
+                                     hist[6], hist[7], smax.c_str());
+                    }
                     // zero-step check: FP64 Rayleigh quotient and residual of the
                     // FP32 Ritz vectors; accepted problems need no FP64 steps
                     const int n_prob = k.n_sectors * b->nsp;
@@ -2329,6 +2366,10 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                         k_brq_accept<<<rg2, rb2, 0, st>>>(a, n_prob, b->n_sets, Eq.p, r2.p, sums.p + n_prob, gapb.p, tol64,
                                                           restart_gap_cap(), ok.p, act_d.p);
                         check_launch("rq check");
+                        if (trace_on()) {
+                            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+                            std::fprintf(stderr, "[qmb batch] rq kernels done at %.2f ms\n", solve_ms());
+                        }
                         Eq.download(e_rq.data(), n_prob, st);
                         act_d.download(act.data(), k.n_sectors, st);
                         QMB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -2371,6 +2412,14 @@ extern "C" qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const dou
                         p2.theta.assign(n_prob, 0.0);
                         p2.conv.assign(n_prob, 1);
                         p2.msteps.assign(n_prob, 0);
+                    }
+                    if (trace_on() && any) {
+                        int hist[8] = {0};
+                        for (int s = 0; s < k.n_sectors; ++s)
+                            for (int set = 0; set < b->n_sets; ++set)
+                                hist[std::min(7, p2.msteps[(size_t)s * b->nsp + set] / 8)]++;
+                        std::fprintf(stderr, "[qmb batch] restart steps per problem 0-7..56+: %d %d %d %d %d %d %d %d\n",
+                                     hist[0], hist[1], hist[2], hist[3], hist[4], hist[5], hist[6], hist[7]);
                     }
                     // sectors that skipped the restart keep the Rayleigh quotient
                     for (int s = 0; s < k.n_sectors; ++s)

@@ -299,6 +299,11 @@ __global__ void k_residual(Op op, const P* __restrict__ psi, double theta, LzDev
 }
 
 // ------------------------------------------------------------------- host
+static int lz_ring_max() {
+    const char* e = std::getenv("QMB_LZ_RING_MAX");
+    return e ? std::max(0, std::atoi(e)) : 0;
+}
+
 int lz_blocks() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -343,6 +348,7 @@ struct PhaseOut {
     double theta = 0.0;
     double est = 0.0;     // residual estimate beta_m |s_{m-1}|
     bool converged = false;
+    bool stored = false;   // v_0 .. v_{m-1} are all in the ring (else the Ritz vector is regenerated)
     bool stalled = false;  // theta stopped moving at the FP32 floor
     double gap = 0.0;      // theta_2 - theta_1 of the last check
     std::vector<double> s_start;  // Ritz coefficients of the restart vector
@@ -385,10 +391,13 @@ struct PhaseOpts {
 
 // Runs one Lanczos phase for operator op with vectors of type V.
 // start_mode 0/1: generated from seed, 2: copied from `from` (type P).
-// With `store` the basis is kept for the Ritz vector (and any
-// reorthogonalisation): the ring starts with the slots the hint asks for
-// (the previous phase's steps plus a check block) and doubles, its filled
-// slots copied over, before a block of steps would wrap it.
+// With `store` the basis is kept for the Ritz vector: the ring starts with
+// the slots the hint asks for (the previous phase's steps plus a check block)
+// and doubles, its filled slots copied over, before a block of steps would
+// wrap it.  A ring that may not grow further (the doubled ring would not fit
+// in free memory) wraps from then on and out.stored is false: the caller
+// regenerates the basis for the Ritz vector.  Reorthogonalisation needs the
+// whole basis, so its ring is allocated in full up front.
 template <class Op, class V, class P>
 PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_mode,
                    uint64_t seed, const P* from, bool store, GrowBuf<V>& vring, int& K,
@@ -400,6 +409,13 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
     const int K_full = store ? cap + 1 : 2;
     const int hint = po.ring_hint ? *po.ring_hint : 0;
     K = store ? std::min(K_full, std::max({hint, 2 + std::max(1, po.check_every), 32})) : 2;
+    // a ring kept from an earlier solve is used to its full size
+    if (store) K = std::min(K_full, std::max(K, (int)(vring.bytes->n / ((size_t)n * sizeof(V)))));
+    // QMB_LZ_RING_MAX caps the ring (tests of the wrapping ring)
+    const int ring_max = lz_ring_max();
+    if (store && ring_max > 0) K = std::max(2, std::min(K, ring_max));
+    if (po.reorth) K = K_full;
+    bool wrapped = false;
     vring.alloc((size_t)K * n);
     wbuf.alloc(2 * (size_t)n);
     st.init(cap, lz_blocks(), po.reorth > 0);
@@ -454,19 +470,24 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
     const int every = std::max(1, po.check_every);
     while (done < cap) {
         int todo = std::min(every, cap - done);
-        if (store && done + todo > K) {
-            // steps done .. done+todo-1 write slots j: grow the ring first
+        if (store && !wrapped && done + todo > K) {
+            // steps done .. done+todo-1 write slots j: grow the ring first,
+            // or let it wrap when the doubled ring does not fit
             const int K2 = std::min(K_full, std::max(2 * K, done + todo));
-            DevBuf<unsigned char> grown;
-            grown.alloc((size_t)K2 * n * sizeof(V));
-            QMB_CUDA_TRY(cudaMemcpyAsync(grown.p, vring.p, (size_t)done * n * sizeof(V),
-                                         cudaMemcpyDeviceToDevice, s));
-            QMB_CUDA_TRY(cudaStreamSynchronize(s));
-            std::swap(vring.bytes->p, grown.p);
-            std::swap(vring.bytes->n, grown.n);
-            vring.p = reinterpret_cast<V*>(vring.bytes->p);
-            K = K2;
-            capture();
+            if ((ring_max > 0 && K2 > ring_max) || !fits_device((size_t)K2 * n * sizeof(V))) {
+                wrapped = true;
+            } else {
+                DevBuf<unsigned char> grown;
+                grown.alloc((size_t)K2 * n * sizeof(V));
+                QMB_CUDA_TRY(cudaMemcpyAsync(grown.p, vring.p, (size_t)done * n * sizeof(V),
+                                             cudaMemcpyDeviceToDevice, s));
+                QMB_CUDA_TRY(cudaStreamSynchronize(s));
+                std::swap(vring.bytes->p, grown.p);
+                std::swap(vring.bytes->n, grown.n);
+                vring.p = reinterpret_cast<V*>(vring.bytes->p);
+                K = K2;
+                capture();
+            }
         }
         for (int t = 0; t < todo; ++t) {
             if (exec) QMB_CUDA_TRY(cudaGraphLaunch(exec, s));
@@ -552,7 +573,8 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
         have_prev = true;
     }
     if (po.tol <= 0) out.converged = true;
-    if (store && po.ring_hint) *po.ring_hint = std::max(*po.ring_hint, out.m + 1 + every);
+    out.stored = store && !wrapped;
+    if (out.stored && po.ring_hint) *po.ring_hint = std::max(*po.ring_hint, out.m + 1 + every);
     out.a.assign(ha.begin(), ha.begin() + out.m);
     out.e.assign(hb.begin() + 1, hb.begin() + out.m);
     if (exec) cudaGraphExecDestroy(exec);
@@ -647,13 +669,13 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     // full FP64 solve from the seeded start vector
     po.ring_hint = &h->lz_ring_hint;
     auto fp64_solve = [&]() {
-        bool store = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap + 3) * n);
+        bool store = o.reorth > 0 ? fits_device(sizeof(V64) * (size_t)(cap + 3) * n) : fits_device(sizeof(V64) * 35 * n);
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
         GrowBuf<V64> vr(&h->lz_ring), wb(&h->lz_wbuf);
         int K;
         last = run_phase<Op64, V64, V64>(op64, sm64, po, o.start, o.seed, nullptr, store, vr, K, wb, st, s);
         n_hv += last.n_hv;
-        ritz_vector<Op64, V64, V64>(op64, sm64, last, o.start, o.seed, nullptr, store, vr, K, wb, st,
+        ritz_vector<Op64, V64, V64>(op64, sm64, last, o.start, o.seed, nullptr, last.stored, vr, K, wb, st,
                                     psi.p, n_hv, s);
         theta = last.theta;
         iters += last.m;
@@ -677,7 +699,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
                 p1.stall_tol = 2e-7;
             }
         }
-        bool store = o.reorth > 0 || fits_device(sizeof(V32) * (size_t)(cap + 3) * n);
+        bool store = o.reorth > 0 ? fits_device(sizeof(V32) * (size_t)(cap + 3) * n) : fits_device(sizeof(V32) * 35 * n);
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
         PhaseOut ph1;
         {
@@ -685,7 +707,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
             int K;
             ph1 = run_phase<Op32, V32, V64>(op32, sm32, p1, o.start, o.seed, nullptr, store, vr, K, wb, st, s);
             n_hv += ph1.n_hv;
-            ritz_vector<Op32, V32, V64>(op32, sm32, ph1, o.start, o.seed, nullptr, store, vr, K, wb,
+            ritz_vector<Op32, V32, V64>(op32, sm32, ph1, o.start, o.seed, nullptr, ph1.stored, vr, K, wb,
                                         st, psi.p, n_hv, s, o.mode == QMB_MODE_MIXED);
         }
         res->E0_low = ph1.theta;
@@ -702,7 +724,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
             p2.check_every = 4;
             p2.gap_in = ph1.gap;
             int cap2 = std::max(1, p2.max_iter);
-            bool store2 = o.reorth > 0 || fits_device(sizeof(V64) * (size_t)(cap2 + 3) * n);
+            bool store2 = o.reorth > 0 ? fits_device(sizeof(V64) * (size_t)(cap2 + 3) * n) : fits_device(sizeof(V64) * 35 * n);
             DevBuf<V64> start(n);
             QMB_CUDA_TRY(cudaMemcpyAsync(start.p, psi.p, sizeof(V64) * n, cudaMemcpyDeviceToDevice, s));
             GrowBuf<V64> vr(&h->lz_ring), wb(&h->lz_wbuf);
@@ -710,7 +732,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
             PhaseOut ph2 = run_phase<Op64, V64, V64>(op64, sm64, p2, 2, 0, start.p, store2, vr, K,
                                                      wb, st, s);
             n_hv += ph2.n_hv;
-            ritz_vector<Op64, V64, V64>(op64, sm64, ph2, 2, 0, start.p, store2, vr, K, wb, st,
+            ritz_vector<Op64, V64, V64>(op64, sm64, ph2, 2, 0, start.p, ph2.stored, vr, K, wb, st,
                                         psi.p, n_hv, s);
             theta = ph2.theta;
             iters += ph2.m;

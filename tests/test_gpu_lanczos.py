@@ -89,6 +89,28 @@ def test_matrix_free_solve_matches_stored():
     assert abs(r1.E0 - r2.E0) < 1e-11 * abs(r1.E0)
 
 
+@pytest.mark.parametrize("mode", [A.MODE_FP64, A.MODE_MIXED])
+def test_wrapping_ring_regenerates_the_basis(mode, monkeypatch):
+    """A Krylov ring that may not grow (QMB_LZ_RING_MAX=4 slots) wraps and
+    the Ritz vector is regenerated from the seed: the energy and the ground
+    state match the solve with the whole basis stored, and the regeneration
+    shows in the product count."""
+    L, k = 16, 8
+    perm, ch = q.translation_group(L)
+    s = q.Sector(L, k, perm).set_irrep(ch[0])
+    h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), [1.0] * L + [0.4] * L, 0.8))
+    r1 = h.lanczos(mode=mode, tol=1e-12, want_vector=1)
+    psi1 = h.ground_state()
+    monkeypatch.setenv("QMB_LZ_RING_MAX", "4")
+    h2 = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), [1.0] * L + [0.4] * L, 0.8))
+    r2 = h2.lanczos(mode=mode, tol=1e-12, want_vector=1)
+    psi2 = h2.ground_state()
+    assert abs(r2.E0 - r1.E0) <= 1e-12 * abs(r1.E0)
+    assert r2.residual < 1e-6 * abs(r1.E0)
+    assert r2.n_hv > r1.n_hv
+    assert abs(abs(np.vdot(psi1, psi2)) - 1.0) < 1e-10
+
+
 def test_ground_state_vector_and_ritz_coefficients():
     L, k = 12, 6
     perm, ch = q.translation_group(L)

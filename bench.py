@@ -155,6 +155,15 @@ def build_batched(q, L=20, n_sets=256):
     return secs, b
 
 
+def time_k1(q, b, prec, reps=20):
+    """The Lanczos step's product kernel as the solve runs it (K1: H x with
+    the epilogue that reads v_{j-1} and writes v_j), CUDA events around each
+    launch inside the library: (ms per step, algorithmic bytes)."""
+    ms, byt = q._capi.C.c_double(), q._capi.C.c_double()
+    q.check(q.lib().qmb_batch_k1_time(b.h, prec, reps, q._capi.C.byref(ms), q._capi.C.byref(byt)))
+    return ms.value, byt.value
+
+
 def time_batch_hv(torch, q, b, prec, reps=20):
     """Average device time of one batched H*v (CUDA events on the launch stream)."""
     off, cp = b.layout()
@@ -577,6 +586,8 @@ def run_batched(args, torch, q, rank, world):
     hv32_ms = time_batch_hv(torch, q, b, A.PREC_FP32)
     hv64_ms = time_batch_hv(torch, q, b, A.PREC_FP64)
     gather = gather_bound(q, b, hv32_ms)
+    k1_32_ms, k1_32_bytes = time_k1(q, b, A.PREC_FP32)
+    k1_64_ms, k1_64_bytes = time_k1(q, b, A.PREC_FP64)
     units = n_sets * L  # sector problems
     ms = float(np.mean(dev_ms))
     value = float(np.mean(hv_count)) / (ms * 1e-3)
@@ -632,9 +643,12 @@ def run_batched(args, torch, q, rank, world):
         "hv_kernel_gbs_fp32": info.bytes_hv_fp32 / (hv32_ms * 1e-3) / 1e9,
         "hv_kernel_gbs_fp64": info.bytes_hv_fp64 / (hv64_ms * 1e-3) / 1e9,
         "hv_ratio_fp32_over_fp64": hv64_ms / hv32_ms,
+        "k1_fp32": {"ms": k1_32_ms, "bytes": k1_32_bytes, "gbs": k1_32_bytes / (k1_32_ms * 1e-3) / 1e9},
+        "k1_fp64": {"ms": k1_64_ms, "bytes": k1_64_bytes, "gbs": k1_64_bytes / (k1_64_ms * 1e-3) / 1e9},
         "gather_bound": gather,
         "max_rel_dE0_mixed_vs_fp64": float(rel.max()),
-        "hv_tuner": {"variant_fp32": int(info.variant_fp32), "variant_fp64": int(info.variant_fp64),
+        "hv_tuner": {"timed": "each variant's K1 (Lanczos-step form) at step 1, minimum of 5 rounds",
+                     "variant_fp32": int(info.variant_fp32), "variant_fp64": int(info.variant_fp64),
                      "ms_fp32": [round(v, 4) for v in info.tune_ms_fp32],
                      "ms_fp64": [round(v, 4) for v in info.tune_ms_fp64],
                      "variants": "k_bhv (slices a thread, unroll, min blocks/SM, hoisted row loads with "
@@ -650,13 +664,15 @@ def run_batched(args, torch, q, rank, world):
         "iters_mixed": [int(r.iters_low), int(r.iters)], "iters_fp64": int(r64.iters),
         "E0_min": float(E_mix.min()),
     }
-    roof_bytes = info.bytes_hv_fp32
     return dict(ms=ms, value=value, units_per_step=float(np.mean(hv_count)), out=out,
                 extra=extra, clocks=clocks, e2e_s=e2e_s,
                 e2e_value=float(np.mean(hv_count)) / e2e_s,
-                h2d=2 * n_sets * 8, d2h=n_sets * L * 8, roof_bytes=roof_bytes, roof_ms=hv32_ms,
+                h2d=2 * n_sets * 8, d2h=n_sets * L * 8, roof_bytes=k1_32_bytes, roof_ms=k1_32_ms,
                 launches=launches,
-                kernel="k_bhv (batched H*v, FP32, one launch per sector kind; the real momenta k=0, 10 are solved in the complex kind)",
+                kernel="k_bhv in the Lanczos step form (K1: y = H w/beta - beta v_{j-1}, v_j stored, alpha "
+                       "summed), FP32, one launch per step over all 20 sectors x 256 sets (the real momenta "
+                       "k=0, 10 are solved in the complex kind); bytes: the product's plus v_{j-1} read and "
+                       "v_j written",
                 dtype="f32+f64")
 
 
@@ -809,6 +825,9 @@ def main():
                     help="two stored FP32 products (k_hv<SellOp<float>>) on the L=28 J1-J2 k=0 even "
                          "sector or the 6x6 k=(0,0) even sector, then exit (the launches the stored-product "
                          "DRAM traffic summary profiles)")
+    ap.add_argument("--profile-k1", action="store_true",
+                    help="build the L=20 batch and time 5 FP32 Lanczos-step products (K1), then exit "
+                         "(the launches the K1 ncu summary profiles)")
     ap.add_argument("--profile-matrix-free", action="store_true",
                     help="two matrix-free FP32 products on the L=32 J1-J2 k=0 even sector, then exit "
                          "(the launch the matrix-free ncu summary profiles)")
@@ -865,6 +884,13 @@ def main():
                           "frac": float(i.bytes_fp32) / (ms * 1e-3) / 1e9 / load_peaks()[0]}))
         return 0
 
+    if args.profile_k1:
+        secs, b = build_batched(q)
+        ms, byt = time_k1(q, b, q._capi.PREC_FP32, reps=5)
+        print(json.dumps({"profile": "K1 (Lanczos-step k_bhv), FP32, L=20 batch, 256 sets", "ms": ms, "bytes": byt,
+                          "frac": byt / (ms * 1e-3) / 1e9 / load_peaks()[0]}))
+        return 0
+
     if args.profile_matrix_free:
         A = q._capi
         L = 32
@@ -908,7 +934,7 @@ def main():
     peak, peak_kind = load_peaks()
     achieved = res["roof_bytes"] / (res["roof_ms"] * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "batched_hv_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "batched_k1_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("traffic_bytes_per_launch")

@@ -475,6 +475,16 @@ QMB_API qmb_status qmb_batch_solve(qmb_batch b, const double* c_xy, const double
  * 16-byte aligned (64-byte alignment, as cudaMalloc gives, lets the fastest
  * kernel variants run). */
 QMB_API qmb_status qmb_batch_hv(qmb_batch b, int prec, const void* x_dev, void* y_dev, void* stream);
+/* Measurement: the batched Lanczos step's product kernel as a solve runs it
+ * (K1: y = H x with the epilogue that reads v_{j-1}, writes v_j and y and
+ * sums alpha), over both sector kinds, on the couplings of the last
+ * qmb_batch_solve (zeros before the first).  reps (1..1000) steps from a
+ * seeded start, each K1 launch bracketed by CUDA events, after one warm-up
+ * step; the steps' update kernels run between them untimed.  *ms = mean K1
+ * time of one step, *bytes = its algorithmic bytes (those of qmb_batch_hv plus
+ * v_{j-1} read and v_j written for every (row, set)).  No reference
+ * counterpart: the reference has no batched solver. */
+QMB_API qmb_status qmb_batch_k1_time(qmb_batch b, int prec, int reps, double* ms, double* bytes);
 /* Device vector layout: sectors of the real kind first, then those of the
  * complex kind (is_complex[s] tells which; real sectors that have fewer than
  * a quarter of the complex sectors' rows are stored and solved complex, with

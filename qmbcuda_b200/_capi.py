@@ -154,6 +154,7 @@ SIGNATURES = {
     "qmb_batch_get_info": (i32, [vp, P(BatchInfo)]),
     "qmb_batch_solve": (i32, [vp, vp, vp, P(LanczosOpts), vp, P(LanczosResult)]),
     "qmb_batch_hv": (i32, [vp, i32, vp, vp, vp]),
+    "qmb_batch_k1_time": (i32, [vp, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "qmb_batch_layout": (i32, [vp, vp, vp]),
 }
 

@@ -800,7 +800,7 @@ struct LoopCtl {
     int reason;   // 1 converged, 2 step cap, 3 compaction, 4 loop bound
     double products;
 };
-__global__ void k_bloop_ctl(cudaGraphConditionalHandle h, int n_sectors, int* __restrict__ active,
+__global__ void k_bloop_ctl(cudaGraphConditionalHandle h, int in_graph, int n_sectors, int* __restrict__ active,
                             int* __restrict__ active_next, int* __restrict__ open_cnt,
                             const int64_t* __restrict__ nrows, const int* __restrict__ weight, int nsp,
                             int check, int cap, const int* __restrict__ iter, int max_loops,
@@ -835,7 +835,7 @@ __global__ void k_bloop_ctl(cudaGraphConditionalHandle h, int n_sectors, int* __
         else if (compact_ratio > 0.0 && cost_c <= compact_ratio * cost_now) { go = 0; reason = 3; }
         else if (ctl->loops >= max_loops) { go = 0; reason = 4; }
         ctl->reason = reason;
-        cudaGraphSetConditional(h, go);
+        if (in_graph) cudaGraphSetConditional(h, go);
     }
 }
 
@@ -1251,6 +1251,15 @@ static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneEntry> g_tune_cache;
 
 template <class V>
+static void bupdate_any(const BatchArgs& a, const BKind& k, V* w, const V* vring, int K, BLz lz, cudaStream_t st);
+template <class V>
+static void bnorm0_any(const BatchArgs& a, const BKind& k, const V* w, BLz lz, cudaStream_t st);
+
+// The variants are timed in the form the solve runs, K1 of a Lanczos step
+// (the product with the epilogue that reads v_{j-1}, writes v_j and y and
+// sums alpha), at step 1 of a seeded start on scratch vectors; the plain
+// product (qmb_batch_hv) uses the same choice.
+template <class V>
 static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st) {
     int& v = k.variant[f64 ? 1 : 0];
     if (v >= 0) return v;
@@ -1279,9 +1288,24 @@ static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st
         }
     }
     const int64_t tot = k.sec_elem[k.n_sectors];
-    DevBuf<V> x(tot), y(tot);
-    QMB_CUDA_TRY(cudaMemsetAsync(x.p, 0, sizeof(V) * tot, st));
-    BLz lz{nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr};
+    const int n_prob = k.n_sectors * a.nsp;
+    DevBuf<V> w(2 * (size_t)tot), ring(2 * (size_t)tot);
+    DevBuf<double> alpha(4 * (size_t)n_prob), beta(5 * (size_t)n_prob),
+        partials((size_t)std::max(1, k.n_tiles) * a.nsp);
+    DevBuf<int> iter(1), act(k.n_sectors);
+    iter.zero(st);
+    std::vector<int> ones(k.n_sectors, 1);
+    act.upload(ones.data(), k.n_sectors, st);
+    BatchArgs at = a;
+    at.active = act.p;  // every sector, whatever the caller's phase has active
+    BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob, k.d_sec_ctr.p, k.d_sec_tile0.p, k.d_sec_ntiles.p};
+    k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(at, tot, 0, 2212456ull, nullptr, w.p);
+    bnorm0_any<V>(at, k, w.p, lz, st);
+    k_bbeta0<<<(n_prob + 255) / 256, 256, 0, st>>>(at, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
+    // one step, so that the timed launches run at step 1 (v_0 read, v_1 written)
+    bhv_variant<V>(0, at, k, w.p, w.p, ring.p, 2, lz, nullptr, nullptr, 1, st);
+    bupdate_any<V>(at, k, w.p, ring.p, 2, lz, st);
+    k_badvance<<<1, 32, 0, st>>>(lz);
     cudaEvent_t e0, e1;
     QMB_CUDA_TRY(cudaEventCreate(&e0));
     QMB_CUDA_TRY(cudaEventCreate(&e1));
@@ -1293,13 +1317,13 @@ static int tuned_variant(const BatchArgs& a, BKind& k, bool f64, cudaStream_t st
     for (int c = 0; c < kBVariants; ++c) {
         tmin[c] = 1e30f;
         fits[c] = bhv_variant_ok<V>(c, a.nsp, spl_for<V>(a.nsp));
-        if (fits[c]) bhv_variant<V>(c, a, k, x.p, y.p, nullptr, 1, lz, nullptr, nullptr, 0, st);  // warm
+        if (fits[c]) bhv_variant<V>(c, at, k, w.p, w.p, ring.p, 2, lz, nullptr, nullptr, 1, st);  // warm
     }
     for (int r = 0; r < 5; ++r)
         for (int c = 0; c < kBVariants; ++c) {
             if (!fits[c]) continue;
             cudaEventRecord(e0, st);
-            bhv_variant<V>(c, a, k, x.p, y.p, nullptr, 1, lz, nullptr, nullptr, 0, st);
+            bhv_variant<V>(c, at, k, w.p, w.p, ring.p, 2, lz, nullptr, nullptr, 1, st);
             cudaEventRecord(e1, st);
             cudaEventSynchronize(e1);
             float ms = 0.f;
@@ -1376,6 +1400,20 @@ static int krylov_slots(size_t vec_bytes, int want, size_t cached = 0) {
 }
 
 // QMB_TRACE=1 prints per-phase steps and times of batched solves to stderr.
+// Compaction threshold: the unconverged problems move to a packed layout
+// once it costs at most this fraction of the current one (QMB_COMPACT_RATIO).
+static double compact_ratio() {
+    const char* e = std::getenv("QMB_COMPACT_RATIO");
+    const double v = e ? std::atof(e) : 0.4;
+    return v > 0.0 && v < 1.0 ? v : 0.4;
+}
+
+// QMB_HOST_LOOP=1: device loops launched block by block from the host
+static bool host_loop() {
+    const char* e = std::getenv("QMB_HOST_LOOP");
+    return e && e[0] == '1';
+}
+
 static bool trace_on() {
     static int v = -1;
     if (v < 0) {
@@ -1434,6 +1472,31 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
     open_cnt.zero(st);
     QMB_CUDA_TRY(cudaMemsetAsync(active_next, 0, sizeof(int) * n_sectors, st));
     const int max_loops = (cap - j0) / check + 1;
+    if (host_loop()) {
+        // the same blocks launched from the host, with the loop control read
+        // back after each (QMB_HOST_LOOP=1: every kernel visible to a profiler)
+        LoopCtl hc{};
+        for (;;) {
+            for (int t = 0; t < check; ++t) step(st);
+            launch_check(a, lz, nsets, stall, res_tol, e_tol, gap_in, gap_out, theta, theta_prev, msteps, conv,
+                         active_next, cap, st, open_cnt.p);
+            g_kernels += 1;
+            k_bloop_ctl<<<1, 256, 0, st>>>(cudaGraphConditionalHandle{}, 0, n_sectors, active, active_next,
+                                           open_cnt.p, d_nrows, d_weight, a.nsp, check, cap, lz.iter, max_loops,
+                                           compact_ratio, ctl.p);
+            check_launch("host loop block");
+            QMB_CUDA_TRY(cudaMemcpyAsync(&hc, ctl.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+            if (hc.reason != 0) break;
+        }
+        int it = 0;
+        QMB_CUDA_TRY(cudaMemcpyAsync(&it, lz.iter, sizeof(int), cudaMemcpyDeviceToHost, st));
+        QMB_CUDA_TRY(cudaStreamSynchronize(st));
+        out.done = it;
+        out.reason = hc.reason;
+        out.products = hc.products;
+        return out;
+    }
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ex = nullptr;
     struct GG {
@@ -1463,7 +1526,7 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
     launch_check(a, lz, nsets, stall, res_tol, e_tol, gap_in, gap_out, theta, theta_prev, msteps, conv,
                  active_next, cap, st, open_cnt.p);
     g_kernels += 1;
-    k_bloop_ctl<<<1, 256, 0, st>>>(h, n_sectors, active, active_next, open_cnt.p, d_nrows, d_weight, a.nsp,
+    k_bloop_ctl<<<1, 256, 0, st>>>(h, 1, n_sectors, active, active_next, open_cnt.p, d_nrows, d_weight, a.nsp,
                                    check, cap, lz.iter, max_loops, compact_ratio, ctl.p);
     cudaGraph_t captured = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &captured);
@@ -1780,7 +1843,7 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             const int cap_run = K < K_full ? std::min(cap, K - 1) : cap;
             lo = device_loop(step, a, lz, b->n_sets, stall, res_tol, e_tol, gap_in, gap_out, theta.p,
                              theta_prev.p, msteps.p, conv.p, k.d_active.p, active_next.p, k.d_nrows.p, d_w.p,
-                             k.n_sectors, std::max(1, check), j0, cap_run, can_compact ? 0.4 : 0.0, st);
+                             k.n_sectors, std::max(1, check), j0, cap_run, can_compact ? compact_ratio() : 0.0, st);
             out.products += lo.products;
             n_hv += lo.done - j0;
             j0 = lo.done;
@@ -2108,6 +2171,8 @@ extern "C" qmb_status qmb_batch_create(const qmb_batch_desc* d, qmb_batch* out) 
         }
         b->cxy.alloc(b->nsp);
         b->cz.alloc(b->nsp);
+        b->cxy.zero();
+        b->cz.zero();
         QMB_CUDA_TRY(cudaDeviceSynchronize());
         if (trace_on())
             std::fprintf(stderr, "[qmb batch] create: sector matrices %.1f ms, device CSR %.1f ms, "
@@ -2222,6 +2287,84 @@ extern "C" qmb_status qmb_batch_hv(qmb_batch b, int prec, const void* x_dev, voi
             batch_hv_kind<float>(b, b->kind[0], false, (const float*)xc, (float*)yc, st);
             batch_hv_kind<float2>(b, b->kind[1], false, (const float2*)(xc + r_elems * rs), (float2*)(yc + r_elems * rs), st);
         }
+    });
+}
+
+namespace qmb {
+// K1 of `reps` Lanczos steps of one kind from a seeded start, each launch
+// bracketed by events; the steps' K2 and advance run between them untimed.
+template <class V>
+static double k1_kind_ms(qmb_batch_s* b, BKind& k, bool f64, int reps, cudaStream_t st) {
+    if (!k.n_sectors || !k.n_tiles) return 0.0;
+    const int64_t tot = k.sec_elem[k.n_sectors];
+    const int n_prob = k.n_sectors * b->nsp;
+    const int cap = reps + 2;
+    DevBuf<V> w(2 * (size_t)tot), ring(2 * (size_t)tot);
+    DevBuf<double> alpha((size_t)(cap + 1) * n_prob), beta((size_t)(cap + 2) * n_prob),
+        partials((size_t)k.n_tiles * b->nsp);
+    DevBuf<int> iter(1);
+    iter.zero(st);
+    std::vector<int> ones(k.n_sectors, 1);
+    k.d_active.upload(ones.data(), k.n_sectors, st);
+    BatchArgs a = make_args(b, k);
+    a.val = f64 ? k.val64.p : k.val32.p;
+    a.dxy = f64 ? k.dxy64.p : k.dxy32.p;
+    a.dz = f64 ? k.dz64.p : k.dz32.p;
+    BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob, k.d_sec_ctr.p, k.d_sec_tile0.p, k.d_sec_ntiles.p};
+    const int rb = 256, rg = (n_prob + rb - 1) / rb;
+    tuned_variant<V>(a, k, f64, st);
+    k_bstart<V><<<grid_for(tot, 256), 256, 0, st>>>(a, tot, 0, 2212456ull, nullptr, w.p);
+    bnorm0_any<V>(a, k, w.p, lz, st);
+    k_bbeta0<<<rg, rb, 0, st>>>(a, k.d_sec_tile0.p, k.d_sec_ntiles.p, lz);
+    std::vector<cudaEvent_t> ev(2 * (size_t)(reps + 1));
+    for (auto& e : ev) QMB_CUDA_TRY(cudaEventCreate(&e));
+    struct EvG {
+        std::vector<cudaEvent_t>& v;
+        ~EvG() { for (auto e : v) cudaEventDestroy(e); }
+    } evg{ev};
+    for (int j = 0; j <= reps; ++j) {  // step 0 warms up
+        QMB_CUDA_TRY(cudaEventRecord(ev[2 * j], st));
+        bhv_any<V>(a, k, w.p, w.p, ring.p, 2, lz, nullptr, nullptr, 1, st);
+        QMB_CUDA_TRY(cudaEventRecord(ev[2 * j + 1], st));
+        bupdate_any<V>(a, k, w.p, ring.p, 2, lz, st);
+        k_badvance<<<1, 32, 0, st>>>(lz);
+    }
+    check_launch("k1 timing");
+    QMB_CUDA_TRY(cudaStreamSynchronize(st));
+    double ms = 0.0;
+    for (int j = 1; j <= reps; ++j) {
+        float t = 0.0f;
+        QMB_CUDA_TRY(cudaEventElapsedTime(&t, ev[2 * j], ev[2 * j + 1]));
+        ms += t;
+    }
+    return ms / reps;
+}
+}  // namespace qmb
+
+extern "C" qmb_status qmb_batch_k1_time(qmb_batch b, int prec, int reps, double* ms, double* bytes) {
+    return guarded([&] {
+        QMB_REQUIRE(b && ms && bytes, QMB_ERR_INVALID, "null argument");
+        QMB_REQUIRE(prec == QMB_PREC_FP64 || prec == QMB_PREC_FP32, QMB_ERR_INVALID, "bad prec");
+        QMB_REQUIRE(reps >= 1 && reps <= 1000, QMB_ERR_INVALID, "reps must be in 1..1000");
+        DeviceGuard dg(b->device);
+        const bool f64 = prec == QMB_PREC_FP64;
+        cudaStream_t st;
+        QMB_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct SG { cudaStream_t s; ~SG() { cudaStreamDestroy(s); } } sg{st};
+        double t = 0.0;
+        if (f64) {
+            t += k1_kind_ms<double>(b, b->kind[0], true, reps, st);
+            t += k1_kind_ms<double2>(b, b->kind[1], true, reps, st);
+        } else {
+            t += k1_kind_ms<float>(b, b->kind[0], false, reps, st);
+            t += k1_kind_ms<float2>(b, b->kind[1], false, reps, st);
+        }
+        // the product's bytes, plus v_{j-1} read and v_j written per (row, set)
+        double extra = 0.0;
+        for (int kd = 0; kd < 2; ++kd)
+            extra += 2.0 * (double)b->kind[kd].rows * b->n_sets * (f64 ? 8.0 : 4.0) * (kd ? 2 : 1);
+        *ms = t;
+        *bytes = batch_bytes(b, f64) + extra;
     });
 }
 

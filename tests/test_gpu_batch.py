@@ -145,6 +145,34 @@ def test_batch_ring_growth_bit_identical(monkeypatch):
     assert max(ring1) >= lo1 + 1 and max(ring1) <= 2 * (lo1 + 10), (ring1, lo1)
 
 
+@pytest.mark.parametrize("mode", [A.MODE_FP64, A.MODE_MIXED])
+def test_host_loop_matches_device_loop(mode, monkeypatch):
+    """QMB_HOST_LOOP=1 launches the device loops' blocks from the host (for
+    profilers, which do not see inside conditional graphs): the same kernels
+    in the same order, so the energies are bit-identical, with and without
+    the compacted tail (200 sets spread the convergence steps)."""
+    L, n_sets = 12, 200
+    bonds = q.chain_bonds(L)
+    rng = np.random.default_rng(7)
+    D = rng.uniform(0, 2, n_sets)
+    J = rng.uniform(0.5, 1.5, n_sets)
+    out = []
+    for host in (None, "1"):
+        if host is None:
+            monkeypatch.delenv("QMB_HOST_LOOP", raising=False)
+        else:
+            monkeypatch.setenv("QMB_HOST_LOOP", host)
+        secs, perm, ch = _sectors(L)
+        b = q.Batch(secs, q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"),
+                    n_sets)
+        E, r = b.solve(J, J * D, mode=mode, max_iter=300, tol=1e-12, seed=5)
+        out.append((E, r.iters, r.iters_low, r.n_products))
+        b.close()
+    (E0, it0, lo0, p0), (E1, it1, lo1, p1) = out
+    assert np.array_equal(E0.view(np.uint64), E1.view(np.uint64))
+    assert (it0, lo0, p0) == (it1, lo1, p1)
+
+
 def test_batch_real_sectors_alone_and_in_complex_kind():
     """Real sectors form their own kind when the batch has no complex ones,
     and join the complex kind when they are a small part of it (L=12: two

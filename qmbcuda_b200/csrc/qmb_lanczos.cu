@@ -408,9 +408,32 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
     int cap = std::max(1, po.max_iter);
     const int K_full = store ? cap + 1 : 2;
     const int hint = po.ring_hint ? *po.ring_hint : 0;
-    K = store ? std::min(K_full, std::max({hint, 2 + std::max(1, po.check_every), 32})) : 2;
+    const int every_steps = std::max(1, po.check_every);
+    // memory the ring may take: the ring kept from earlier solves (reused)
+    // plus free memory, less a reserve for the vectors a solve allocates
+    // besides (work vectors, start and Ritz vectors in the high precision)
+    const size_t slot = (size_t)n * sizeof(V);
+    const size_t reserve = 6 * (size_t)n * sizeof(P) + ((size_t)256 << 20);
+    auto free_bytes = [&]() {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return (size_t)0;
+        }
+        return fr;
+    };
+    K = store ? std::min(K_full, std::max({hint, 2 + every_steps, 32})) : 2;
     // a ring kept from an earlier solve is used to its full size
-    if (store) K = std::min(K_full, std::max(K, (int)(vring.bytes->n / ((size_t)n * sizeof(V)))));
+    if (store) K = std::min(K_full, std::max(K, (int)(vring.bytes->n / slot)));
+    if (store && !po.reorth) {
+        const size_t avail = vring.bytes->n + free_bytes();
+        const int K_fit = avail > reserve ? (int)std::min<size_t>((avail - reserve) / slot, (size_t)K_full) : 0;
+        K = std::min(K, K_fit);
+        if (K < 2 + every_steps) {  // not even one block of steps: regenerate instead
+            store = false;
+            K = 2;
+        }
+    }
     // QMB_LZ_RING_MAX caps the ring (tests of the wrapping ring)
     const int ring_max = lz_ring_max();
     if (store && ring_max > 0) K = std::max(2, std::min(K, ring_max));
@@ -474,7 +497,8 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
             // steps done .. done+todo-1 write slots j: grow the ring first,
             // or let it wrap when the doubled ring does not fit
             const int K2 = std::min(K_full, std::max(2 * K, done + todo));
-            if ((ring_max > 0 && K2 > ring_max) || !fits_device((size_t)K2 * n * sizeof(V))) {
+            // the grown ring is allocated while the current one is held
+            if ((ring_max > 0 && K2 > ring_max) || (size_t)K2 * slot + reserve > free_bytes()) {
                 wrapped = true;
             } else {
                 DevBuf<unsigned char> grown;
@@ -669,7 +693,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
     // full FP64 solve from the seeded start vector
     po.ring_hint = &h->lz_ring_hint;
     auto fp64_solve = [&]() {
-        bool store = o.reorth > 0 ? fits_device(sizeof(V64) * (size_t)(cap + 3) * n) : fits_device(sizeof(V64) * 35 * n);
+        bool store = o.reorth > 0 ? fits_device(sizeof(V64) * (size_t)(cap + 3) * n) : true;
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
         GrowBuf<V64> vr(&h->lz_ring), wb(&h->lz_wbuf);
         int K;
@@ -699,7 +723,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
                 p1.stall_tol = 2e-7;
             }
         }
-        bool store = o.reorth > 0 ? fits_device(sizeof(V32) * (size_t)(cap + 3) * n) : fits_device(sizeof(V32) * 35 * n);
+        bool store = o.reorth > 0 ? fits_device(sizeof(V32) * (size_t)(cap + 3) * n) : true;
         QMB_REQUIRE(o.reorth == 0 || store, QMB_ERR_NOMEM, "Krylov basis does not fit for reorthogonalisation");
         PhaseOut ph1;
         {
@@ -724,7 +748,7 @@ void solve(qmb_ham_s* h, const Op32& op32, size_t sm32, const Op64& op64, size_t
             p2.check_every = 4;
             p2.gap_in = ph1.gap;
             int cap2 = std::max(1, p2.max_iter);
-            bool store2 = o.reorth > 0 ? fits_device(sizeof(V64) * (size_t)(cap2 + 3) * n) : fits_device(sizeof(V64) * 35 * n);
+            bool store2 = o.reorth > 0 ? fits_device(sizeof(V64) * (size_t)(cap2 + 3) * n) : true;
             DevBuf<V64> start(n);
             QMB_CUDA_TRY(cudaMemcpyAsync(start.p, psi.p, sizeof(V64) * n, cudaMemcpyDeviceToDevice, s));
             GrowBuf<V64> vr(&h->lz_ring), wb(&h->lz_wbuf);

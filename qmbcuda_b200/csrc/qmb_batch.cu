@@ -1918,7 +1918,9 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             }
         if (te[0]) QMB_CUDA_TRY(cudaEventRecord(te[0], st));
         g_kernels += 1;
-        k_britz<<<rg, rb, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p, gap_out);
+        // one thread per problem, long serial loops: 32-thread blocks spread
+        // the problems over every SM (5,120 problems are 20 blocks of 256)
+        k_britz<<<(n_prob + 31) / 32, 32, 0, st>>>(lz, msteps.p, theta.p, Ls.p, Ds.p, xs.p, ritz.p, gap_out);
         if (te[1]) QMB_CUDA_TRY(cudaEventRecord(te[1], st));
         if (K > 2 && done < K) {
             g_kernels += 1;

@@ -233,10 +233,11 @@ typedef struct {
     int64_t padded;        /* sliced-ELL slots including padding */
     int max_row;           /* largest off-diagonal count of a row */
     int is_complex;
-    int n_codes;           /* distinct off-diagonal values (dictionary size) */
-    int coded;             /* 1: off-diagonals packed as 8-bit code | 24-bit column */
-    double bytes_fp64;     /* algorithmic bytes of one FP64 H*v */
-    double bytes_fp32;     /* algorithmic bytes of one FP32 H*v */
+    int n_codes;           /* distinct off-diagonal FP32 values (dictionary size) */
+    int coded;             /* 1: FP32 off-diagonals packed as 8-bit code | 24-bit column */
+    double bytes_fp64;     /* algorithmic bytes of one FP64 H*v (plain sliced-ELL entries) */
+    double bytes_fp32;     /* algorithmic bytes of one FP32 H*v (plain sliced-ELL entries) */
+    int coded_fp64;        /* 1: real FP64 off-diagonals packed the same way (one block) */
 } qmb_ham_info;
 
 /* Builds the matrix on the active rows of the sector's irrep, in sliced ELL

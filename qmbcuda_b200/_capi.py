@@ -62,7 +62,8 @@ class Terms(C.Structure):
 class HamInfo(C.Structure):
     _fields_ = [("n_rows", C.c_int64), ("nnz_offdiag", C.c_int64), ("padded", C.c_int64),
                 ("max_row", C.c_int), ("is_complex", C.c_int), ("n_codes", C.c_int),
-                ("coded", C.c_int), ("bytes_fp64", C.c_double), ("bytes_fp32", C.c_double)]
+                ("coded", C.c_int), ("bytes_fp64", C.c_double), ("bytes_fp32", C.c_double),
+                ("coded_fp64", C.c_int)]
 
 
 class LanczosOpts(C.Structure):

@@ -25,7 +25,7 @@ namespace qmb {
 // (SZ and identity operators) or one SP and one SM at two distinct sites with
 // nothing else; otherwise n_hops = 0 and the operator runs the general term
 // loop.  Hops on the same two sites merge, per direction.
-static void hop_form(qmb_ham_s* h, const qmb_terms* t) {
+void hop_form(qmb_ham_s* h, const qmb_terms* t) {
     h->n_hops = 0;
     std::vector<Hop> hp;
     std::vector<double2> cf;
@@ -306,6 +306,8 @@ void build_sell(qmb_ham_s* h) {
 constexpr int kCbMaxBlocks = 32;                     // column blocks at most
 constexpr size_t kCbBlockBytes = (size_t)64 << 20;   // x bytes of one column block
 constexpr double kCbMinVecBytes = 256.0 * (1 << 20); // vectors from this size on (2x L2)
+constexpr double kCbMinStreamBytes = 256.0 * (1 << 20);  // single block: plain entries (8 B) from this size on
+constexpr double kCbMaxSingleVecBytes = 96.0 * (1 << 20);  // single FP64 block: x bytes up to this (L2 126 MB)
 constexpr int kCbMissCap = 1024;                     // values outside the dictionary kept per pass
 
 // Bit pattern of a matrix value (the dictionary key).
@@ -313,7 +315,9 @@ __device__ __forceinline__ uint64_t val_key(float v) { return __float_as_uint(v)
 __device__ __forceinline__ uint64_t val_key(float2 v) {
     return ((uint64_t)__float_as_uint(v.y) << 32) | __float_as_uint(v.x);
 }
+__device__ __forceinline__ uint64_t val_key(double v) { return (uint64_t)__double_as_longlong(v); }
 __device__ __forceinline__ bool val_zero(float v) { return v == 0.0f; }
+__device__ __forceinline__ bool val_zero(double v) { return v == 0.0; }
 __device__ __forceinline__ bool val_zero(float2 v) { return v.x == 0.0f && v.y == 0.0f; }
 
 // Every stride-th slot of the sliced ELL's FP32 values (dictionary sample).
@@ -427,18 +431,20 @@ static void cb_skip(const char* why) {
 }
 
 template <class M>
-static void build_cb_t(qmb_ham_s* h, int forced_shift) {
+static void build_cb_t(qmb_ham_s* h, int forced_shift, bool single, CbLayout& L) {
+    constexpr bool f64 = sizeof(typename Sc<M>::real) == 8;
     const int64_t n = h->n;
     const size_t es = sizeof(M);
     int shift = 24;
-    while (shift > 10 && ((size_t)1 << shift) * es > kCbBlockBytes) --shift;
+    if (!single)
+        while (shift > 10 && ((size_t)1 << shift) * es > kCbBlockBytes) --shift;
     if (forced_shift) shift = forced_shift;
     const int nb = (int)((n + ((int64_t)1 << shift) - 1) >> shift);
-    if (nb < 2 || nb > kCbMaxBlocks || h->max_row > 255) {
+    if (nb < (single ? 1 : 2) || nb > (single ? 1 : kCbMaxBlocks) || h->max_row > 255) {
         cb_skip("block count or row length out of range");
         return;
     }
-    SellOp<M> a = h->sell<M>(false);
+    SellOp<M> a = h->sell<M>(f64);
     // dictionary from a strided sample of the values
     const int64_t n_samp = std::min<int64_t>(h->padded, (int64_t)1 << 20);
     const int64_t stride = std::max<int64_t>(1, h->padded / n_samp);
@@ -453,7 +459,10 @@ static void build_cb_t(qmb_ham_s* h, int forced_shift) {
         std::sort(hs.begin(), hs.end());
         hs.erase(std::unique(hs.begin(), hs.end()), hs.end());
         for (uint64_t k : hs) {
-            const bool zero = es == 4 ? ((uint32_t)k << 1) == 0 : (((uint32_t)k << 1) == 0 && ((uint32_t)(k >> 32) << 1) == 0);
+            // +-0 in every component
+            const bool zero = f64 ? (k << 1) == 0
+                                  : es == 4 ? ((uint32_t)k << 1) == 0
+                                            : (((uint32_t)k << 1) == 0 && ((uint32_t)(k >> 32) << 1) == 0);
             if (!zero) keys.push_back(k);
         }
     }
@@ -527,18 +536,23 @@ static void build_cb_t(qmb_ham_s* h, int forced_shift) {
     std::vector<M> dict(256);
     std::memset(dict.data(), 0, sizeof(M) * 256);
     for (size_t i = 0; i < keys.size(); ++i) std::memcpy(&dict[i + 1], &keys[i], sizeof(M));
-    h->cb_dict.alloc(256 * sizeof(M));
-    QMB_CUDA_TRY(cudaMemcpy(h->cb_dict.p, dict.data(), 256 * sizeof(M), cudaMemcpyHostToDevice));
-    h->cb_ytmp.alloc((size_t)n * (h->cplx ? 16 : 8));
-    h->cb_off = std::move(off);
-    h->cb_width = std::move(width);
-    h->cb_packed = std::move(packed);
-    h->cb_nb = nb;
-    h->cb_shift = shift;
-    h->n_codes = (int)keys.size();
+    L.dict.alloc(256 * sizeof(M));
+    QMB_CUDA_TRY(cudaMemcpy(L.dict.p, dict.data(), 256 * sizeof(M), cudaMemcpyHostToDevice));
+    if (nb > 1) L.ytmp.alloc((size_t)n * (h->cplx ? 16 : 8));
+    L.off = std::move(off);
+    L.width = std::move(width);
+    L.packed = std::move(packed);
+    L.nb = nb;
+    L.shift = shift;
+    L.n_codes = (int)keys.size();
     QMB_CUDA_TRY(cudaDeviceSynchronize());
 }
 
+//
+// The same layout with one block (every column in the 24-bit field) serves a
+// matrix whose vectors fit L2 but whose entry stream is large (the plain FP32
+// entries, 8 or 12 bytes, at least kCbMinStreamBytes): its 32-bit coded entries
+// halve (real) or third (complex) the bytes a product streams.
 //
 // QMB_CB_SHIFT=s (10..24) builds the layout with blocks of 2^s rows for any
 // matrix with at least two blocks, whatever its size (small cases exercise
@@ -552,9 +566,18 @@ void build_cb(qmb_ham_s* h) {
         const int v = std::atoi(e);
         if (v >= 10 && v <= 24) forced = v;
     }
-    if (!forced && (double)h->n * (h->cplx ? 8 : 4) < kCbMinVecBytes) return;
-    if (h->cplx) build_cb_t<float2>(h, forced);
-    else build_cb_t<float>(h, forced);
+    const bool blocked = (double)h->n * (h->cplx ? 8 : 4) >= kCbMinVecBytes;
+    const bool single = !blocked && h->n <= ((int64_t)1 << 24) &&
+                        (double)h->padded * (h->cplx ? 12 : 8) >= kCbMinStreamBytes;
+    if (forced || blocked || single) {
+        if (h->cplx) build_cb_t<float2>(h, forced, single && !forced, h->cb32);
+        else build_cb_t<float>(h, forced, single && !forced, h->cb32);
+    }
+    // real FP64 values: one block when x (8 bytes a row) stays well inside L2
+    // and the plain entries (12 bytes) stream at least kCbMinStreamBytes
+    if ((h->prec & QMB_PREC_FP64) && h->val64.p && !h->cplx && (double)h->n * 8 <= kCbMaxSingleVecBytes &&
+        (double)h->padded * 12 >= kCbMinStreamBytes)
+        build_cb_t<double>(h, 0, true, h->cb64);
 }
 
 // Row-order copies for the matrix-free lookup: each row's representative
@@ -709,8 +732,9 @@ extern "C" qmb_status qmb_ham_get_info(qmb_ham h, qmb_ham_info* info) {
         info->padded = h->padded;
         info->max_row = h->max_row;
         info->is_complex = h->cplx ? 1 : 0;
-        info->n_codes = h->n_codes;
-        info->coded = h->cb_nb > 0 ? 1 : 0;
+        info->n_codes = h->cb32.n_codes;
+        info->coded = h->cb32.nb > 0 ? 1 : 0;
+        info->coded_fp64 = h->cb64.nb > 0 ? 1 : 0;
         double vs64 = h->cplx ? 16 : 8, vs32 = h->cplx ? 8 : 4;
         // compulsory traffic: index + value per off-diagonal, diagonal value,
         // x read once, y written once
@@ -795,11 +819,12 @@ void hv_dispatch(const qmb_ham_s* h, int prec, const void* x, void* y, cudaStrea
                 "the handle does not hold values of the requested precision");
     if (h->cplx) {
         if (f64) launch_hv(h->sell<double2>(true), (const double2*)x, (double2*)y, st, 0);
-        else if (h->cb_nb > 0) launch_hv(h->cb<float2>(), (const float2*)x, (float2*)y, st, CbSellOp<float2>::smem_bytes());
+        else if (h->cb32.nb > 0) launch_hv(h->cb<float2>(), (const float2*)x, (float2*)y, st, CbSellOp<float2>::smem_bytes());
         else launch_hv(h->sell<float2>(false), (const float2*)x, (float2*)y, st, 0);
     } else {
-        if (f64) launch_hv(h->sell<double>(true), (const double*)x, (double*)y, st, 0);
-        else if (h->cb_nb > 0) launch_hv(h->cb<float>(), (const float*)x, (float*)y, st, CbSellOp<float>::smem_bytes());
+        if (f64 && h->cb64.nb > 0) launch_hv(h->cb<double>(), (const double*)x, (double*)y, st, CbSellOp<double>::smem_bytes());
+        else if (f64) launch_hv(h->sell<double>(true), (const double*)x, (double*)y, st, 0);
+        else if (h->cb32.nb > 0) launch_hv(h->cb<float>(), (const float*)x, (float*)y, st, CbSellOp<float>::smem_bytes());
         else launch_hv(h->sell<float>(false), (const float*)x, (float*)y, st, 0);
     }
 }

@@ -232,17 +232,20 @@ struct SellOp {
     }
 };
 
-// Column-blocked coded sliced ELL (FP32 values), for sectors whose vector
-// is larger than L2: the columns are split into nb blocks of 2^shift rows and
-// every block has its own sliced ELL (32-row slices, column-major inside a
-// slice) whose 32-bit entries pack an 8-bit value code (into a dictionary of
-// at most 255 FP32 values; code 0 is the padding, value 0) above the 24-bit
-// column inside the block.  A product makes one pass per block in block
+// Column-blocked coded sliced ELL: the columns are split into nb blocks of
+// 2^shift rows and every block has its own sliced ELL (32-row slices,
+// column-major inside a slice) whose 32-bit entries pack an 8-bit value code
+// (into a dictionary of at most 255 values; code 0 is the padding, value 0)
+// above the 24-bit column inside the block.  For sectors whose vector is
+// larger than L2 (FP32 values) a product makes one pass per block in block
 // order, so the part of x a pass gathers from (one block, at most 64 MB)
 // stays in L2 while the matrix streams from HBM once: passes 0 .. nb-2
 // (pre(), k_cb_pass) leave partial row sums in ytmp, and the last pass is
-// row(), which adds its block and hands the row to the calling kernel.
-template <class M>  // float or float2
+// row(), which adds its block and hands the row to the calling kernel.  A
+// single block (nb = 1) serves matrices whose vector fits L2 but whose entry
+// stream is large (FP32, and real FP64 values): 4 bytes an entry instead of
+// 8 or 12.
+template <class M>  // float, float2 or double
 struct CbSellOp {
     int64_t n;
     int nb;                 // column blocks
@@ -438,6 +441,17 @@ struct ActiveLookup {
 constexpr int kMaxHops = 512;
 struct Hop {
     uint64_t pair;  // bits i < j; direction 0 raises site i (bit i zero, bit j one)
+};
+
+// A coded layout of a matrix's stored values in one precision (CbSellOp):
+// per column block a sliced ELL of 32-bit entries, an 8-bit code into a
+// dictionary of at most 255 values above the column inside the block.
+struct CbLayout {
+    int nb = 0, shift = 0, n_codes = 0;
+    DevBuf<int64_t> off;
+    DevBuf<int> width;
+    DevBuf<uint32_t> packed;
+    DevBuf<unsigned char> dict, ytmp;
 };
 
 // Matrix-free operator: regenerates every entry of the row.  pre() writes
@@ -640,12 +654,9 @@ struct qmb_ham_s {
     qmb::DevBuf<int> slice_w;
     qmb::DevBuf<uint32_t> col;        // plain columns
     qmb::DevBuf<unsigned char> val64, val32, diag64, diag32;
-    // column-blocked coded FP32 layout (CbSellOp), built for vectors larger than L2
-    int cb_nb = 0, cb_shift = 0, n_codes = 0;
-    qmb::DevBuf<int64_t> cb_off;
-    qmb::DevBuf<int> cb_width;
-    qmb::DevBuf<uint32_t> cb_packed;
-    qmb::DevBuf<unsigned char> cb_dict, cb_ytmp;
+    // coded layouts of the stored values (CbSellOp): FP32 (column-blocked for
+    // vectors larger than L2, else one block) and real FP64 (one block)
+    qmb::CbLayout cb32, cb64;
     // terms kept for the matrix-free operator
     int n_terms = 0, n_col = 0;
     qmb::DevBuf<int> t_nops;
@@ -709,17 +720,19 @@ struct qmb_ham_s {
         return op;
     }
     template <class M> qmb::CbSellOp<M> cb() const {
+        constexpr bool f64 = sizeof(typename qmb::Sc<M>::real) == 8;
+        const qmb::CbLayout& L = f64 ? cb64 : cb32;
         qmb::CbSellOp<M> op;
         op.n = n;
-        op.nb = cb_nb;
-        op.shift = cb_shift;
+        op.nb = L.nb;
+        op.shift = L.shift;
         op.n_slices = n_slices;
-        op.off = cb_off.p;
-        op.width = cb_width.p;
-        op.packed = cb_packed.p;
-        op.dict = reinterpret_cast<const M*>(cb_dict.p);
-        op.diag = reinterpret_cast<const M*>(diag32.p);
-        op.ytmp = cb_ytmp.p;
+        op.off = L.off.p;
+        op.width = L.width.p;
+        op.packed = L.packed.p;
+        op.dict = reinterpret_cast<const M*>(L.dict.p);
+        op.diag = reinterpret_cast<const M*>(f64 ? diag64.p : diag32.p);
+        op.ytmp = L.ytmp.p;
         op.sdict = nullptr;
         return op;
     }
@@ -754,6 +767,10 @@ struct qmb_ham_s {
 namespace qmb {
 // Builds the matrix-free operator's tables on the handle (once).
 void mf_tables(qmb_ham_s* h);
+// The hop form of a validated term table (for the matrix-free operator).
+void hop_form(qmb_ham_s* h, const qmb_terms* t);
+// The coded FP32 layout of a built matrix, when it pays (CbSellOp).
+void build_cb(qmb_ham_s* h);
 // Upload operator tables (validated) into the handle's term buffers.
 void upload_terms(qmb_ham_s* h, const qmb_terms* t, int L);
 int grid_for(int64_t n, int block);

@@ -841,51 +841,45 @@ extern "C" qmb_status qmb_lanczos(qmb_ham h, const qmb_lanczos_opts* opts, qmb_l
         } else {
             mf_tables(h);
         }
-        if (h->cplx) {
-            if (mf) {
-                auto a = h->mf<float2>();
-                auto b = h->mf<double2>();
-                solve<MfOp<float2>, MfOp<double2>, float2, double2>(h, a, a.smem_bytes(), b, b.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
-            } else if (!need32) {
-                auto b = h->sell<double2>(true);
-                solve<SellOp<double2>, SellOp<double2>, float2, double2>(h, b, 0, b, 0, o, res, krylov_coeffs, n_coeffs);
-            } else if (!need64) {
-                if (h->cb_nb > 0) {
-                    auto a = h->cb<float2>();
-                    solve<CbSellOp<float2>, CbSellOp<float2>, float2, double2>(h, a, a.smem_bytes(), a, a.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
-                } else {
-                    auto a = h->sell<float2>(false);
-                    solve<SellOp<float2>, SellOp<float2>, float2, double2>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
+        // operators: matrix-free, or the stored values in the coded layout
+        // where one was built, else the plain sliced ELL; the low phase's
+        // operator is unused in FP64 mode and stands in for the high one in
+        // FP32 mode
+        auto dispatch = [&](auto real_tag) {
+            using R = decltype(real_tag);  // float or float2
+            using D = typename std::conditional<std::is_same<R, float>::value, double, double2>::type;
+            auto run = [&](const auto& a, size_t sa, const auto& b, size_t sb) {
+                using A = typename std::decay<decltype(a)>::type;
+                using B = typename std::decay<decltype(b)>::type;
+                solve<A, B, R, D>(h, a, sa, b, sb, o, res, krylov_coeffs, n_coeffs);
+            };
+            auto op32 = [&](auto&& k) {
+                if (h->cb32.nb > 0) k(h->cb<R>(), CbSellOp<R>::smem_bytes());
+                else k(h->sell<R>(false), (size_t)0);
+            };
+            auto op64 = [&](auto&& k) {
+                if constexpr (std::is_same<D, double>::value) {
+                    if (h->cb64.nb > 0) {
+                        k(h->cb<D>(), CbSellOp<D>::smem_bytes());
+                        return;
+                    }
                 }
-            } else if (h->cb_nb > 0) {
-                auto a = h->cb<float2>();
-                solve<CbSellOp<float2>, SellOp<double2>, float2, double2>(h, a, a.smem_bytes(), h->sell<double2>(true), 0, o, res, krylov_coeffs, n_coeffs);
-            } else {
-                solve<SellOp<float2>, SellOp<double2>, float2, double2>(h, h->sell<float2>(false), 0, h->sell<double2>(true), 0, o, res, krylov_coeffs, n_coeffs);
-            }
-        } else {
+                k(h->sell<D>(true), (size_t)0);
+            };
             if (mf) {
-                auto a = h->mf<float>();
-                auto b = h->mf<double>();
-                solve<MfOp<float>, MfOp<double>, float, double>(h, a, a.smem_bytes(), b, b.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
+                auto a = h->mf<R>();
+                auto b = h->mf<D>();
+                run(a, a.smem_bytes(), b, b.smem_bytes());
             } else if (!need32) {
-                auto b = h->sell<double>(true);
-                solve<SellOp<double>, SellOp<double>, float, double>(h, b, 0, b, 0, o, res, krylov_coeffs, n_coeffs);
+                op64([&](const auto& b, size_t sb) { run(b, sb, b, sb); });
             } else if (!need64) {
-                if (h->cb_nb > 0) {
-                    auto a = h->cb<float>();
-                    solve<CbSellOp<float>, CbSellOp<float>, float, double>(h, a, a.smem_bytes(), a, a.smem_bytes(), o, res, krylov_coeffs, n_coeffs);
-                } else {
-                    auto a = h->sell<float>(false);
-                    solve<SellOp<float>, SellOp<float>, float, double>(h, a, 0, a, 0, o, res, krylov_coeffs, n_coeffs);
-                }
-            } else if (h->cb_nb > 0) {
-                auto a = h->cb<float>();
-                solve<CbSellOp<float>, SellOp<double>, float, double>(h, a, a.smem_bytes(), h->sell<double>(true), 0, o, res, krylov_coeffs, n_coeffs);
+                op32([&](const auto& a, size_t sa) { run(a, sa, a, sa); });
             } else {
-                solve<SellOp<float>, SellOp<double>, float, double>(h, h->sell<float>(false), 0, h->sell<double>(true), 0, o, res, krylov_coeffs, n_coeffs);
+                op32([&](const auto& a, size_t sa) { op64([&](const auto& b, size_t sb) { run(a, sa, b, sb); }); });
             }
-        }
+        };
+        if (h->cplx) dispatch(float2{});
+        else dispatch(float{});
         if (!res->converged && o.tol > 0) throw Error{QMB_ERR_NOT_CONVERGED, "Lanczos did not reach the tolerance within max_iter"};
     });
 }

@@ -436,10 +436,33 @@ extern "C" qmb_status qmb_ham_load(qmb_sector s, const char* path, qmb_ham* out)
         }
         upload<int>(h->t_nops, tn, (size_t)h->n_terms);
         upload<uint16_t>(h->t_ops, to, (size_t)h->n_terms * h->n_col);
-        upload<double2>(h->t_scalar, F.get(TAG_T_SCALAR, 16, (uint64_t)h->n_terms), (size_t)h->n_terms);
+        const double2* tsc = (const double2*)F.get(TAG_T_SCALAR, 16, (uint64_t)h->n_terms);
+        upload<double2>(h->t_scalar, tsc, (size_t)h->n_terms);
+        {
+            // the hop form, as qmb_ham_create derives it from the same table
+            std::vector<int> codes((size_t)h->n_terms * h->n_col), sites(codes.size());
+            std::vector<double> sc(2 * (size_t)h->n_terms);
+            for (size_t i = 0; i < codes.size(); ++i) {
+                codes[i] = to[i] >> 8;
+                sites[i] = to[i] & 0xff;
+            }
+            for (int i = 0; i < h->n_terms; ++i) {
+                sc[2 * (size_t)i] = tsc[i].x;
+                sc[2 * (size_t)i + 1] = tsc[i].y;
+            }
+            qmb_terms t{};
+            t.n_terms = h->n_terms;
+            t.n_col = h->n_col;
+            t.n_ops = tn;
+            t.op_code = codes.data();
+            t.op_site = sites.data();
+            t.scalar = sc.data();
+            hop_form(h.get(), &t);
+        }
         h->err.alloc(1);
         h->err.zero();
         QMB_CUDA_TRY(cudaDeviceSynchronize());
+        build_cb(h.get());  // the coded FP32 layout, as qmb_ham_create builds it
         *out = h.release();
     });
 }

@@ -192,6 +192,44 @@ def test_matrix_free_active_lookup(L, k, flip, a):
     assert abs(r_mf.E0 - r_st.E0) <= 1e-10 * abs(r_st.E0)
 
 
+def test_single_block_coded_layout(monkeypatch):
+    """A matrix whose vectors fit L2 but whose FP32 entry stream exceeds
+    256 MB (L=30 J1-J2, k=0 even: 2.6 M rows) gets the coded layout with one
+    column block (32-bit entries: an 8-bit value code above the column), for
+    its FP32 and its FP64 values: the products equal the plain sliced-ELL
+    products to FP32 / FP64 rounding, and a mixed solve on it equals the FP64
+    energy."""
+    import torch
+    L = 30
+    perm, ch = q.translation_group(L)
+    s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+    terms = q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), [1.0] * L + [0.45] * L, [0.9] * L + [0.4] * L)
+    h = q.Hamiltonian(s, terms)
+    assert h.info.coded == 1 and h.info.coded_fp64 == 1
+    monkeypatch.setenv("QMB_COLUMN_BLOCKS", "0")
+    hp = q.Hamiltonian(s, terms)
+    assert hp.info.coded == 0 and hp.info.coded_fp64 == 0
+    n = int(h.info.n_rows)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randn(n, dtype=torch.float32, device="cuda", generator=g)
+    y1, y2 = torch.empty_like(x), torch.empty_like(x)
+    h.hv_dev(x.data_ptr(), y1.data_ptr(), q._capi.PREC_FP32)
+    hp.hv_dev(x.data_ptr(), y2.data_ptr(), q._capi.PREC_FP32)
+    torch.cuda.synchronize()
+    assert float((y1 - y2).abs().max()) <= 2e-6 * float(y2.abs().max())
+    # the FP64 values coded the same way: the products agree to FP64 rounding
+    x64 = x.double()
+    z1, z2 = torch.empty_like(x64), torch.empty_like(x64)
+    h.hv_dev(x64.data_ptr(), z1.data_ptr(), q._capi.PREC_FP64)
+    hp.hv_dev(x64.data_ptr(), z2.data_ptr(), q._capi.PREC_FP64)
+    torch.cuda.synchronize()
+    assert float((z1 - z2).abs().max()) <= 1e-13 * float(z2.abs().max())
+    A = q._capi
+    r64 = h.lanczos(mode=A.MODE_FP64, tol=1e-12)
+    rmx = h.lanczos(mode=A.MODE_MIXED, tol=1e-12)
+    assert abs(rmx.E0 - r64.E0) <= 1e-9 * abs(r64.E0)
+
+
 @pytest.mark.parametrize("a", [0, 3])
 def test_column_blocked_product_and_solve(a, monkeypatch):
     """The column-blocked coded FP32 layout (built for vectors larger than L2;

@@ -856,7 +856,7 @@ def main():
                     help="time only the batched H*v kernels (small device footprint, for profiling)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison solve and the end-to-end repeat")
-    ap.add_argument("--profile-stored", choices=["l28", "6x6"], default=None,
+    ap.add_argument("--profile-stored", choices=["l28", "l32", "l32-fp64", "6x6"], default=None,
                     help="two stored FP32 products (k_hv<SellOp<float>>) on the L=28 J1-J2 k=0 even "
                          "sector or the 6x6 k=(0,0) even sector, then exit (the launches the stored-product "
                          "DRAM traffic summary profiles)")
@@ -894,29 +894,32 @@ def main():
             s = q.Sector(N * N, N * N // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
             terms = q.xxz_terms(q.square_bonds(N, N), 1.0, 1.0)
         else:
-            L = 28
+            L = 28 if args.profile_stored == "l28" else 32
             perm, ch = q.translation_group(L)
             s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
             J = [1.0] * L + [0.5] * L
             terms = q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J)
-        h = q.Hamiltonian(s, terms, prec=A.PREC_FP32)
-        x = torch.randn(int(h.info.n_rows), dtype=torch.float32, device="cuda")
+        f64 = args.profile_stored == "l32-fp64"
+        prec = A.PREC_FP64 if f64 else A.PREC_FP32
+        h = q.Hamiltonian(s, terms, prec=prec)
+        x = torch.randn(int(h.info.n_rows), dtype=torch.float64 if f64 else torch.float32, device="cuda")
         y = torch.empty_like(x)
         for _ in range(2):
-            q.check(q.lib().qmb_hv(h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None))
+            q.check(q.lib().qmb_hv(h.h, prec, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None))
         torch.cuda.synchronize()
         i = h.info
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(3):
-            q.check(q.lib().qmb_hv(h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None))
+            q.check(q.lib().qmb_hv(h.h, prec, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None))
         e1.record()
         e1.synchronize()
         ms = e0.elapsed_time(e1) / 3
-        print(json.dumps({"profile": f"stored FP32 product, {args.profile_stored}", "rows": int(i.n_rows),
-                          "nnz": int(i.nnz_offdiag), "bytes_fp32": float(i.bytes_fp32),
-                          "column_blocked": int(i.coded), "ms": ms,
-                          "frac": float(i.bytes_fp32) / (ms * 1e-3) / 1e9 / load_peaks()[0]}))
+        byt, ell = fp64_product_bytes(i) if f64 else fp32_product_bytes(i)
+        print(json.dumps({"profile": f"stored {'FP64' if f64 else 'FP32'} product, {args.profile_stored}",
+                          "rows": int(i.n_rows), "nnz": int(i.nnz_offdiag), "bytes": byt, "bytes_ell_convention": ell,
+                          "coded": int(i.coded_fp64 if f64 else i.coded), "ms": ms,
+                          "frac": byt / (ms * 1e-3) / 1e9 / load_peaks()[0]}))
         return 0
 
     if args.profile_k1:

@@ -558,7 +558,6 @@ static void build_cb_t(qmb_ham_s* h, int forced_shift, bool single, CbLayout& L)
 // matrix with at least two blocks, whatever its size (small cases exercise
 // the layout in tests).
 void build_cb(qmb_ham_s* h) {
-    if (!(h->prec & QMB_PREC_FP32) || !h->val32.p) return;
     if (const char* e = std::getenv("QMB_COLUMN_BLOCKS"))
         if (e[0] == '0') return;
     int forced = 0;
@@ -569,7 +568,7 @@ void build_cb(qmb_ham_s* h) {
     const bool blocked = (double)h->n * (h->cplx ? 8 : 4) >= kCbMinVecBytes;
     const bool single = !blocked && h->n <= ((int64_t)1 << 24) &&
                         (double)h->padded * (h->cplx ? 12 : 8) >= kCbMinStreamBytes;
-    if (forced || blocked || single) {
+    if ((h->prec & QMB_PREC_FP32) && h->val32.p && (forced || blocked || single)) {
         if (h->cplx) build_cb_t<float2>(h, forced, single && !forced, h->cb32);
         else build_cb_t<float>(h, forced, single && !forced, h->cb32);
     }

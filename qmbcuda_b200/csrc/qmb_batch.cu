@@ -804,7 +804,8 @@ __global__ void k_bloop_ctl(cudaGraphConditionalHandle h, int in_graph, int n_se
                             int* __restrict__ active_next, int* __restrict__ open_cnt,
                             const int64_t* __restrict__ nrows, const int* __restrict__ weight, int nsp,
                             int check, int cap, const int* __restrict__ iter, int max_loops,
-                            double compact_ratio, LoopCtl* __restrict__ ctl) {
+                            double compact_ratio, const int* __restrict__ group, int n_groups,
+                            LoopCtl* __restrict__ ctl) {
     __shared__ double red[32];
     double prev_w = 0.0, any = 0.0, cost_now = 0.0, cost_c = 0.0;
     for (int s = threadIdx.x; s < n_sectors; s += blockDim.x) {
@@ -813,7 +814,21 @@ __global__ void k_bloop_ctl(cudaGraphConditionalHandle h, int in_graph, int n_se
         any += an;
         if (an) {
             cost_now += (double)nrows[s] * nsp;
-            cost_c += (double)nrows[s] * 32.0 * (double)((open_cnt[s] + 31) / 32);
+            if (!group) cost_c += (double)nrows[s] * 32.0 * (double)((open_cnt[s] + 31) / 32);
+        }
+    }
+    if (group) {
+        // a compacted sub-batch: the open problems of all its virtual sectors
+        // over one base sector (group) would share the packed sectors
+        for (int g = threadIdx.x; g < n_groups; g += blockDim.x) {
+            int open = 0;
+            int64_t rows = 0;
+            for (int s = 0; s < n_sectors; ++s)
+                if (group[s] == g && active_next[s]) {
+                    open += open_cnt[s];
+                    rows = nrows[s];
+                }
+            cost_c += (double)rows * 32.0 * (double)((open + 31) / 32);
         }
     }
     prev_w = block_sum(prev_w, red);
@@ -923,54 +938,50 @@ __global__ void k_britz(BLz lz, const int* __restrict__ msteps, const double* __
 
 // dst[v][r][q] = src[vs_base[v]][r][vs_set[v][q]], one block per tile of 32 rows.
 template <class V>
-__global__ void k_bgather_vec(BatchArgs ac, const int* __restrict__ vs_base, const int* __restrict__ vs_set,
-                              const int64_t* __restrict__ sec_elem_b, int nsp_b, const V* __restrict__ src,
-                              V* __restrict__ dst) {
+__global__ void k_bgather_vec(BatchArgs ac, const int* __restrict__ slot_src, const int64_t* __restrict__ sec_elem_s,
+                              int nsp_s, const V* __restrict__ src, V* __restrict__ dst) {
     const int tile = blockIdx.x;
     const int v = ac.tile_sector[tile];
     const int nsp_c = ac.nsp;
     const int q = threadIdx.x % nsp_c;
-    const int set = vs_set[v * nsp_c + q];
-    const int64_t eb = sec_elem_b[vs_base[v]], ec = ac.sec_elem[v];
+    const int sp = slot_src[v * nsp_c + q];  // source problem: source sector * nsp_s + set
+    const int64_t eb = sec_elem_s[sp / nsp_s] + sp % nsp_s, ec = ac.sec_elem[v];
     const int64_t r_end = min(ac.sec_nrows[v], (int64_t)ac.tile_row0[tile] + kBTile);
     for (int64_t r = ac.tile_row0[tile] + threadIdx.x / nsp_c; r < r_end; r += blockDim.x / nsp_c)
-        dst[ec + r * nsp_c + q] = src[eb + r * nsp_b + set];
+        dst[ec + r * nsp_c + q] = src[eb + r * nsp_s];
 }
 
 // alpha_i (i < j), beta_i (i <= j) and the convergence-test state of the
-// migrated problems.
-__global__ void k_bgather_state(int n_prob_c, int nsp_c, int nsp_b, int n_prob_b, int j,
-                                const int* __restrict__ vs_base, const int* __restrict__ vs_set,
-                                const int* __restrict__ real_c, const double* __restrict__ alpha_b,
-                                const double* __restrict__ beta_b, const double* __restrict__ thp_b,
-                                const int* __restrict__ ms_b, const double* __restrict__ gap_b,
+// migrated problems; slot_src maps a slot to its source problem.
+__global__ void k_bgather_state(int n_prob_c, int n_prob_s, int j, const int* __restrict__ slot_src,
+                                const int* __restrict__ real_c, const double* __restrict__ alpha_s,
+                                const double* __restrict__ beta_s, const double* __restrict__ thp_s,
+                                const int* __restrict__ ms_s, const double* __restrict__ gap_s,
                                 double* __restrict__ alpha_c, double* __restrict__ beta_c,
                                 double* __restrict__ thp_c, int* __restrict__ ms_c, double* __restrict__ gap_c,
                                 int* __restrict__ conv_c) {
     for (int pc = blockIdx.x * blockDim.x + threadIdx.x; pc < n_prob_c; pc += gridDim.x * blockDim.x) {
-        const int v = pc / nsp_c;
-        const int p = vs_base[v] * nsp_b + vs_set[pc];
-        for (int i = 0; i < j; ++i) alpha_c[(int64_t)i * n_prob_c + pc] = alpha_b[(int64_t)i * n_prob_b + p];
-        for (int i = 0; i <= j; ++i) beta_c[(int64_t)i * n_prob_c + pc] = beta_b[(int64_t)i * n_prob_b + p];
-        thp_c[pc] = thp_b[p];
-        ms_c[pc] = ms_b[p];
-        if (gap_b) gap_c[pc] = gap_b[p];
+        const int p = slot_src[pc];
+        for (int i = 0; i < j; ++i) alpha_c[(int64_t)i * n_prob_c + pc] = alpha_s[(int64_t)i * n_prob_s + p];
+        for (int i = 0; i <= j; ++i) beta_c[(int64_t)i * n_prob_c + pc] = beta_s[(int64_t)i * n_prob_s + p];
+        thp_c[pc] = thp_s[p];
+        ms_c[pc] = ms_s[p];
+        if (gap_s) gap_c[pc] = gap_s[p];
         conv_c[pc] = real_c[pc] ? 0 : 1;
     }
 }
 
-// Results of the real slots back into the base problem arrays.
-__global__ void k_bscatter_state(int n_prob_c, int nsp_c, int nsp_b, const int* __restrict__ vs_base,
-                                 const int* __restrict__ vs_set, const int* __restrict__ real_c,
+// Results of the real slots back into the source problem arrays.
+__global__ void k_bscatter_state(int n_prob_c, const int* __restrict__ slot_src, const int* __restrict__ real_c,
                                  const double* __restrict__ th_c, const int* __restrict__ ms_c,
-                                 const int* __restrict__ conv_c, double* __restrict__ th_b,
-                                 int* __restrict__ ms_b, int* __restrict__ conv_b) {
+                                 const int* __restrict__ conv_c, double* __restrict__ th_s,
+                                 int* __restrict__ ms_s, int* __restrict__ conv_s) {
     for (int pc = blockIdx.x * blockDim.x + threadIdx.x; pc < n_prob_c; pc += gridDim.x * blockDim.x) {
         if (!real_c[pc]) continue;
-        const int p = vs_base[pc / nsp_c] * nsp_b + vs_set[pc];
-        th_b[p] = th_c[pc];
-        ms_b[p] = ms_c[pc];
-        conv_b[p] = conv_c[pc];
+        const int p = slot_src[pc];
+        th_s[p] = th_c[pc];
+        ms_s[p] = ms_c[pc];
+        conv_s[p] = conv_c[pc];
     }
 }
 
@@ -1408,6 +1419,18 @@ static double compact_ratio() {
     return v > 0.0 && v < 1.0 ? v : 0.4;
 }
 
+// The threshold inside a compacted sub-batch (QMB_SUB_COMPACT_RATIO, off by
+// default): its virtual sectors over one base sector merge into fewer.  On
+// the L=20 batch (34 virtual sectors over 20 base sectors after the first
+// compaction) further levels (34 -> 24 -> 19 sectors at thresholds up to
+// 0.85) cost as much in host round trips and gathers as their smaller tail
+// saved: 110-116 ms against 110 ms per mixed solve.
+static double sub_compact_ratio() {
+    const char* e = std::getenv("QMB_SUB_COMPACT_RATIO");
+    const double v = e ? std::atof(e) : 0.0;
+    return v > 0.0 && v < 1.0 ? v : 0.0;
+}
+
 // QMB_HOST_LOOP=1: device loops launched block by block from the host
 static bool host_loop() {
     const char* e = std::getenv("QMB_HOST_LOOP");
@@ -1463,7 +1486,8 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
                            double res_tol, double e_tol, const double* gap_in, double* gap_out, double* theta,
                            double* theta_prev, int* msteps, int* conv, int* active, int* active_next,
                            const int64_t* d_nrows, const int* d_weight, int n_sectors, int check, int j0,
-                           int cap, double compact_ratio, cudaStream_t st) {
+                           int cap, double compact_ratio, cudaStream_t st, const int* d_group = nullptr,
+                           int n_groups = 0) {
     LoopOut out{j0, 2, 0.0};
     if (j0 + check > cap) return out;
     Buf<LoopCtl> ctl = ws_take<LoopCtl>(1);
@@ -1483,7 +1507,7 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
             g_kernels += 1;
             k_bloop_ctl<<<1, 256, 0, st>>>(cudaGraphConditionalHandle{}, 0, n_sectors, active, active_next,
                                            open_cnt.p, d_nrows, d_weight, a.nsp, check, cap, lz.iter, max_loops,
-                                           compact_ratio, ctl.p);
+                                           compact_ratio, d_group, n_groups, ctl.p);
             check_launch("host loop block");
             QMB_CUDA_TRY(cudaMemcpyAsync(&hc, ctl.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
             QMB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1527,7 +1551,7 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
                  active_next, cap, st, open_cnt.p);
     g_kernels += 1;
     k_bloop_ctl<<<1, 256, 0, st>>>(h, 1, n_sectors, active, active_next, open_cnt.p, d_nrows, d_weight, a.nsp,
-                                   check, cap, lz.iter, max_loops, compact_ratio, ctl.p);
+                                   check, cap, lz.iter, max_loops, compact_ratio, d_group, n_groups, ctl.p);
     cudaGraph_t captured = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &captured);
     QMB_CUDA_TRY(ce);
@@ -1547,32 +1571,55 @@ static LoopOut device_loop(StepFn&& step, const BatchArgs& a, const BLz& lz, int
     return out;
 }
 
+// A layout the compaction reads the unconverged problems from: the base kind
+// (nsp sets a sector) or an earlier compacted sub-batch (32 slots a virtual
+// sector).  Source sector s lies over base sector base_of[s]; its vectors
+// start at d_sec_elem[s]; problem p = s * nsp + set.
+struct CSrc {
+    int n_sectors = 0, nsp = 0;
+    std::vector<int> base_of;        // [n_sectors]
+    const int64_t* d_sec_elem = nullptr;
+    std::vector<double> cx, cz;      // couplings per source problem
+    std::vector<int> real;           // 1 for a real problem (not padding)
+    const double* alpha = nullptr;   // [j][n_prob] as in BLz
+    const double* beta = nullptr;
+    double* theta = nullptr;
+    double* theta_prev = nullptr;
+    const double* gap = nullptr;     // phase-1 gap per problem, or null
+    int* msteps = nullptr;
+    int* conv = nullptr;
+    int n_prob() const { return n_sectors * nsp; }
+};
+
 // Continues the Lanczos recurrences of the unconverged problems of a phase
 // (K = 2 ring, no Ritz vector wanted) in a compacted sub-batch of 32 slots
-// per virtual sector, from step j up to step cap.  conv_h is the host copy of
-// the base convergence flags after step j.  Results (theta, steps, flags) go
-// back into the base arrays; returns the step count reached.
+// per virtual sector, from step j up to step cap.  src describes the layout
+// they come from (w_j and v_{j-1} at w_src and v_src) and conv_h its
+// convergence flags after step j.  When the unconverged problems of the
+// sub-batch again fill few enough slots, they move on into a smaller one (up
+// to kCompactDepth levels).  Results (theta, steps, flags) go back into the
+// source arrays; returns the step count reached.
+constexpr int kCompactDepth = 3;
 template <class V>
-static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_base, const BLz& lz_base,
-                         V* wbuf, V* vring, int j, int cap, double stall, double res_tol, double e_tol,
-                         const double* gap_in, int check, const std::vector<int>& conv_h,
-                         double* theta_b, double* theta_prev_b, int* msteps_b, int* conv_b,
+static int run_compacted(qmb_batch_s* b, BKind& k, std::unique_ptr<BKind>& holder, bool f64, const BatchArgs& a_base,
+                         const CSrc& src, const V* w_src, const V* v_src, int j, int cap, double stall,
+                         double res_tol, double e_tol, int check, const std::vector<int>& conv_h, int depth,
                          double& products, int& n_hv, cudaStream_t st) {
     constexpr int NC = 32;
-    const int nsp_b = b->nsp;
-    // virtual sectors
-    std::vector<int> vs_base, vs_set, real;
+    // virtual sectors: the open problems of each base sector, 32 a sector
+    std::vector<std::vector<int>> open_of(k.n_sectors);
+    for (int p = 0; p < src.n_prob(); ++p)
+        if (src.real[p] && !conv_h[p]) open_of[src.base_of[p / src.nsp]].push_back(p);
+    std::vector<int> vs_base, slot_src, real;
     std::vector<int> n_real;
     for (int s = 0; s < k.n_sectors; ++s) {
-        std::vector<int> open;
-        for (int set = 0; set < b->n_sets; ++set)
-            if (!conv_h[(size_t)s * nsp_b + set]) open.push_back(set);
+        const std::vector<int>& open = open_of[s];
         for (size_t c = 0; c < open.size(); c += NC) {
             vs_base.push_back(s);
             const int nr = (int)std::min<size_t>(NC, open.size() - c);
             n_real.push_back(nr);
             for (int q = 0; q < NC; ++q) {
-                vs_set.push_back(open[c + std::min(q, nr - 1)]);
+                slot_src.push_back(open[c + std::min(q, nr - 1)]);
                 real.push_back(q < nr ? 1 : 0);
             }
         }
@@ -1580,8 +1627,8 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     const int nv = (int)vs_base.size();
     if (nv == 0) return j;
     // the compacted layout's descriptor is kept on the kind and refilled
-    if (!k.compact) k.compact = std::make_unique<BKind>();
-    BKind& ck = *k.compact;
+    if (!holder) holder = std::make_unique<BKind>();
+    BKind& ck = *holder;
     ck.nrows.clear();
     ck.sec_tile0.clear();
     ck.sec_ntiles.clear();
@@ -1601,6 +1648,7 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
             v = best;
         }
         ck.variant[f] = v;
+        for (int c = 0; c < kBVariants; ++c) ck.tune_ms[f][c] = k.tune_ms[f][c];
     }
     ck.max_tile_entries = k.max_tile_entries;
     std::vector<int64_t> rb(nv), r0(nv);
@@ -1643,22 +1691,16 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     ck.d_ctr.zero(st);
     if (ck.d_sec_ctr.n < (size_t)nv) ck.d_sec_ctr.alloc(nv);
     ck.d_sec_ctr.zero(st);
-    Buf<int> d_vs_base = ws_take<int>(vs_base.size()), d_vs_set = ws_take<int>(vs_set.size()),
-             d_real = ws_take<int>(real.size());
-    d_vs_base.upload(vs_base.data(), vs_base.size(), st);
-    d_vs_set.upload(vs_set.data(), vs_set.size(), st);
+    Buf<int> d_slot_src = ws_take<int>(slot_src.size()), d_real = ws_take<int>(real.size());
+    d_slot_src.upload(slot_src.data(), slot_src.size(), st);
     d_real.upload(real.data(), real.size(), st);
     // couplings of each slot
-    std::vector<double> hx(nsp_b), hz(nsp_b), cx(n_prob_c), cz(n_prob_c);
-    b->cxy.download(hx.data(), nsp_b, st);
-    b->cz.download(hz.data(), nsp_b, st);
-    QMB_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<double> cx(n_prob_c), cz(n_prob_c);
     for (int pc = 0; pc < n_prob_c; ++pc) {
-        cx[pc] = hx[vs_set[pc]];
-        cz[pc] = hz[vs_set[pc]];
+        cx[pc] = src.cx[slot_src[pc]];
+        cz[pc] = src.cz[slot_src[pc]];
     }
-    Buf<double> d_cx = ws_take<double>(n_prob_c),
-        d_cz = ws_take<double>(n_prob_c);
+    Buf<double> d_cx = ws_take<double>(n_prob_c), d_cz = ws_take<double>(n_prob_c);
     d_cx.upload(cx.data(), n_prob_c, st);
     d_cz.upload(cz.data(), n_prob_c, st);
     BatchArgs ac = a_base;  // matrix arrays of the base kind
@@ -1675,15 +1717,12 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
     ac.c_stride = NC;
     ac.active = ck.d_active.p;
     // recurrence state: w_j, v_{j-1}, alpha/beta history, test state
-    const int64_t tot_b = k.sec_elem[k.n_sectors];
-    Buf<V> wc = ws_take<V>(2 * (size_t)tot_c),
-        vc = ws_take<V>(2 * (size_t)tot_c);
+    Buf<V> wc = ws_take<V>(2 * (size_t)tot_c), vc = ws_take<V>(2 * (size_t)tot_c);
     g_kernels += 1;
-    k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
-                                                 wbuf + (int64_t)(j & 1) * tot_b, wc.p + (int64_t)(j & 1) * tot_c);
+    k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_slot_src.p, src.d_sec_elem, src.nsp, w_src,
+                                                 wc.p + (int64_t)(j & 1) * tot_c);
     g_kernels += 1;
-    k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_vs_base.p, d_vs_set.p, k.d_sec_elem.p, nsp_b,
-                                                 vring + (int64_t)((j + 1) & 1) * tot_b,
+    k_bgather_vec<V><<<ck.n_tiles, 256, 0, st>>>(ac, d_slot_src.p, src.d_sec_elem, src.nsp, v_src,
                                                  vc.p + (int64_t)((j + 1) & 1) * tot_c);
     Buf<double> alpha = ws_take<double>((size_t)(cap + 1) * n_prob_c),
         beta = ws_take<double>((size_t)(cap + 2) * n_prob_c),
@@ -1697,8 +1736,8 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
         active_next = ws_take<int>(nv);
     g_kernels += 1;
     k_bgather_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(
-        n_prob_c, NC, nsp_b, lz_base.n_prob, j, d_vs_base.p, d_vs_set.p, d_real.p, lz_base.alpha, lz_base.beta,
-        theta_prev_b, msteps_b, gap_in, alpha.p, beta.p, theta_prev.p, msteps.p, gap.p, conv.p);
+        n_prob_c, src.n_prob(), j, d_slot_src.p, d_real.p, src.alpha, src.beta, src.theta_prev, src.msteps,
+        src.gap, alpha.p, beta.p, theta_prev.p, msteps.p, gap.p, conv.p);
     iter.upload(&j, 1, st);
     check_launch("compaction");
     BLz lz{alpha.p, beta.p, partials.p, iter.p, n_prob_c, ck.d_sec_ctr.p, ck.d_sec_tile0.p, ck.d_sec_ntiles.p};
@@ -1709,20 +1748,47 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
         g_kernels += 1;
         k_badvance<<<1, 32, 0, ss>>>(lz);
     };
+    const double* gap_c = src.gap ? gap.p : nullptr;
     int done = j;
     {
         Buf<int> d_w = ws_take<int>(nv);
         d_w.upload(n_real.data(), nv, st);
-        LoopOut lo = device_loop(step, ac, lz, NC, stall, res_tol, e_tol, gap_in ? gap.p : nullptr, nullptr, theta.p,
-                                 theta_prev.p, msteps.p, conv.p, ck.d_active.p, active_next.p, ck.d_nrows.p, d_w.p,
-                                 nv, std::max(1, check), j, cap, 0.0, st);
+        const double ratio = depth + 1 < kCompactDepth ? sub_compact_ratio() : 0.0;
+        Buf<int> d_group = ws_take<int>(nv);
+        d_group.upload(vs_base.data(), nv, st);
+        LoopOut lo = device_loop(step, ac, lz, NC, stall, res_tol, e_tol, gap_c, nullptr, theta.p, theta_prev.p,
+                                 msteps.p, conv.p, ck.d_active.p, active_next.p, ck.d_nrows.p, d_w.p, nv,
+                                 std::max(1, check), j, cap, ratio, st, d_group.p, k.n_sectors);
         done = lo.done;
         products += lo.products;
         n_hv += done - j;
         if (trace_on())
-            std::fprintf(stderr, "[qmb batch] compacted %s loop: %d virtual sectors, steps %d..%d, stop reason %d\n",
-                         f64 ? "fp64" : "fp32", nv, j, done, lo.reason);
-        if (lo.reason != 1 && done < cap) {
+            std::fprintf(stderr, "[qmb batch] compacted %s loop (level %d): %d virtual sectors, steps %d..%d, stop reason %d\n",
+                         f64 ? "fp64" : "fp32", depth + 1, nv, j, done, lo.reason);
+        if (lo.reason == 3) {
+            // the unconverged problems of this sub-batch move into a smaller one
+            CSrc me;
+            me.n_sectors = nv;
+            me.nsp = NC;
+            me.base_of = vs_base;
+            me.d_sec_elem = ck.d_sec_elem.p;
+            me.cx = cx;
+            me.cz = cz;
+            me.real = real;
+            me.alpha = alpha.p;
+            me.beta = beta.p;
+            me.theta = theta.p;
+            me.theta_prev = theta_prev.p;
+            me.gap = gap_c;
+            me.msteps = msteps.p;
+            me.conv = conv.p;
+            std::vector<int> hc(n_prob_c);
+            conv.download(hc.data(), n_prob_c, st);
+            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+            done = run_compacted<V>(b, k, ck.compact, f64, a_base, me, wc.p + (int64_t)(done & 1) * tot_c,
+                                    vc.p + (int64_t)((done + 1) & 1) * tot_c, done, cap, stall, res_tol, e_tol,
+                                    check, hc, depth + 1, products, n_hv, st);
+        } else if (lo.reason != 1 && done < cap) {
             std::vector<int> act(nv);
             ck.d_active.download(act.data(), nv, st);
             QMB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1734,15 +1800,14 @@ static int run_compacted(qmb_batch_s* b, BKind& k, bool f64, const BatchArgs& a_
             done += rem;
             n_hv += rem;
             QMB_CUDA_TRY(cudaMemsetAsync(active_next.p, 0, sizeof(int) * nv, st));
-            launch_check(ac, lz, NC, stall, res_tol, e_tol, gap_in ? gap.p : nullptr, nullptr, theta.p,
-                         theta_prev.p, msteps.p, conv.p, active_next.p, done, st);
+            launch_check(ac, lz, NC, stall, res_tol, e_tol, gap_c, nullptr, theta.p, theta_prev.p, msteps.p,
+                         conv.p, active_next.p, done, st);
             check_launch("compacted last steps");
         }
     }
     g_kernels += 1;
-    k_bscatter_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(n_prob_c, NC, nsp_b, d_vs_base.p, d_vs_set.p,
-                                                            d_real.p, theta.p, msteps.p, conv.p, theta_b,
-                                                            msteps_b, conv_b);
+    k_bscatter_state<<<(n_prob_c + 255) / 256, 256, 0, st>>>(n_prob_c, d_slot_src.p, d_real.p, theta.p, msteps.p,
+                                                            conv.p, src.theta, src.msteps, src.conv);
     check_launch("compaction results");
     QMB_CUDA_TRY(cudaStreamSynchronize(st));
     return done;
@@ -1877,10 +1942,34 @@ static BPhase run_bphase(qmb_batch_s* b, BKind& k, bool f64, int max_iter, doubl
             std::vector<int> hc(n_prob);
             conv.download(hc.data(), n_prob, st);
             QMB_CUDA_TRY(cudaStreamSynchronize(st));
-            const int j0 = done;
-            done = run_compacted<V>(b, k, f64, a, lz, wbuf.p, vring.p, done, cap, stall, res_tol, e_tol, gap_in,
-                                    check, hc, theta.p, theta_prev.p, msteps.p, conv.p, out.products, n_hv, st);
-            (void)j0;
+            CSrc base;
+            base.n_sectors = k.n_sectors;
+            base.nsp = b->nsp;
+            base.base_of.resize(k.n_sectors);
+            for (int s = 0; s < k.n_sectors; ++s) base.base_of[s] = s;
+            base.d_sec_elem = k.d_sec_elem.p;
+            std::vector<double> hx(b->nsp), hz(b->nsp);
+            b->cxy.download(hx.data(), b->nsp, st);
+            b->cz.download(hz.data(), b->nsp, st);
+            QMB_CUDA_TRY(cudaStreamSynchronize(st));
+            base.cx.resize(n_prob);
+            base.cz.resize(n_prob);
+            base.real.resize(n_prob);
+            for (int p = 0; p < n_prob; ++p) {
+                base.cx[p] = hx[p % b->nsp];
+                base.cz[p] = hz[p % b->nsp];
+                base.real[p] = p % b->nsp < b->n_sets ? 1 : 0;
+            }
+            base.alpha = lz.alpha;
+            base.beta = lz.beta;
+            base.theta = theta.p;
+            base.theta_prev = theta_prev.p;
+            base.gap = gap_in;
+            base.msteps = msteps.p;
+            base.conv = conv.p;
+            done = run_compacted<V>(b, k, k.compact, f64, a, base, wbuf.p + (int64_t)(done & 1) * tot,
+                                    vring.p + (int64_t)((done + 1) & 1) * tot, done, cap, stall, res_tol, e_tol,
+                                    check, hc, 0, out.products, n_hv, st);
         } else if (lo.reason != 1 && done < cap) {
             // the last steps (fewer than a block) with one test at the end
             std::vector<int> act(k.n_sectors);

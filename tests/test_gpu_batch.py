@@ -115,6 +115,37 @@ def test_batch_many_sets_dense_oracle(mode):
         assert err.max() <= tol, (a, err.max(), int(err.argmax()))
 
 
+def test_batch_compaction_levels(monkeypatch):
+    """With QMB_SUB_COMPACT_RATIO=0.9 the unconverged problems of a compacted
+    sub-batch move on into smaller ones (up to three levels); every energy
+    still equals dense diagonalisation of its sector matrix, in FP64 and in
+    mixed mode."""
+    monkeypatch.setenv("QMB_SUB_COMPACT_RATIO", "0.9")
+    L, n_sets = 12, 200
+    secs, perm, ch = _sectors(L)
+    bonds = q.chain_bonds(L)
+    b = q.Batch(secs, q.xxz_terms(bonds, 1.0, 0.0, part="xy"), q.xxz_terms(bonds, 0.0, 1.0, part="z"), n_sets)
+    rng = np.random.default_rng(17)
+    D = rng.uniform(0, 2, n_sets)
+    J = rng.uniform(0.5, 1.5, n_sets)
+    g = oracle_group(perm, ch)
+    sec = O.build_sector(g, L // 2)
+    txy, tz = q.xxz_terms(bonds, 1.0, 0.0), q.xxz_terms(bonds, 0.0, 1.0)
+    e = np.zeros((n_sets, L))
+    for a in range(L):
+        rows = O.active_rows(sec, a)
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(txy), a, 2 * txy.n_terms + 1)
+        Axy = O.ell_to_csr(ind, val, tr, rows).toarray()
+        rc, ind, val, tr = O.ell_terms(sec, oracle_terms(tz), a, 2 * tz.n_terms + 1)
+        Dz = O.ell_to_csr(ind, val, tr, rows).toarray()
+        H = J[:, None, None] * Axy[None] + (J * D)[:, None, None] * Dz[None]
+        e[:, a] = np.linalg.eigvalsh(H)[:, 0]
+    for mode in (A.MODE_FP64, A.MODE_MIXED):
+        E, summ = b.solve(J, J * D, mode=mode, max_iter=300, tol=1e-12)
+        err = np.abs(E - e) / np.maximum(np.abs(e), 1.0)
+        assert err.max() <= 1e-10, (mode, err.max())
+
+
 def test_batch_ring_growth_bit_identical(monkeypatch):
     """A Krylov ring that starts at 4 vectors doubles until the FP32 phase
     fits: the solve is bit-identical to one whose ring held the phase from

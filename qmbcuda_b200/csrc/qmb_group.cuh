@@ -18,6 +18,7 @@ constexpr int kTableSmemMax = 96 * 1024;
 struct GroupArgs {
     int L, G, n_ext, structured, W, n_chunks;
     int full_rot;             // a chain group of all L rotations, element 0 the identity
+    int full_torus;           // all R x W translations of a torus of W-site rows (W <= 8), element 0 the identity
     uint64_t mask;
     const ElemRot* rot;       // [G] device
     const uint64_t* tables;   // [G][n_chunks][16] device
@@ -28,12 +29,14 @@ struct GroupArgs {
 struct GroupSmem {
     const ElemRot* rot;
     const uint64_t* tab;
-    const int* gofr;  // full_rot: the element of each rotation amount
+    const int* gofr;          // full_rot / full_torus: element of translation (a rows, c sites) at a * W + c
+    const uint8_t* minrot;    // full_torus: smallest rotation of each W-bit row value
+    const uint8_t* rotmask;   // full_torus: the rotations reaching it (bit c)
 };
 
 // Bytes of dynamic shared memory a kernel needs for the group.
 __host__ __device__ inline size_t group_smem_bytes(const GroupArgs& g) {
-    if (g.structured) return sizeof(ElemRot) * (size_t)g.G + sizeof(int) * 64;
+    if (g.structured) return sizeof(ElemRot) * (size_t)g.G + sizeof(int) * 64 + 2 * 256;
     size_t t = sizeof(uint64_t) * (size_t)g.G * g.n_chunks * 16;
     return t <= (size_t)kTableSmemMax ? t : 0;
 }
@@ -42,16 +45,36 @@ __host__ __device__ inline size_t group_smem_bytes(const GroupArgs& g) {
 __device__ __forceinline__ GroupSmem load_group(const GroupArgs& g, unsigned char* sm) {
     GroupSmem out;
     out.gofr = nullptr;
+    out.minrot = out.rotmask = nullptr;
     if (g.structured) {
         ElemRot* r = reinterpret_cast<ElemRot*>(sm);
         int* gofr = reinterpret_cast<int*>(r + g.G);
+        uint8_t* minrot = reinterpret_cast<uint8_t*>(gofr + 64);
+        uint8_t* rotmask = minrot + 256;
         for (int i = threadIdx.x; i < g.G; i += blockDim.x) {
             r[i] = g.rot[i];
-            if (g.full_rot) gofr[g.rot[i].ri] = i;
+            if (g.full_rot || g.full_torus) gofr[(int)(g.rot[i].rr / g.W) * g.W + (int)g.rot[i].ri] = i;
         }
+        if (g.full_torus)
+            for (int v = threadIdx.x; v < (1 << g.W); v += blockDim.x) {
+                int best = 1 << g.W, m = 0;
+                for (int c = 0; c < g.W; ++c) {
+                    const int y = c ? (((v << c) | (v >> (g.W - c))) & ((1 << g.W) - 1)) : v;
+                    if (y < best) {
+                        best = y;
+                        m = 1 << c;
+                    } else if (y == best) {
+                        m |= 1 << c;
+                    }
+                }
+                minrot[v] = (uint8_t)best;
+                rotmask[v] = (uint8_t)m;
+            }
         out.rot = r;
         out.tab = g.tables;
         out.gofr = gofr;
+        out.minrot = minrot;
+        out.rotmask = rotmask;
     } else {
         size_t n = (size_t)g.G * g.n_chunks * 16;
         if (n * sizeof(uint64_t) <= (size_t)kTableSmemMax) {
@@ -112,12 +135,18 @@ __device__ __forceinline__ uint32_t apply_site_map32(const GroupArgs& g, const G
 
 __device__ __forceinline__ uint32_t chain_orbit_min(const GroupArgs& g, const GroupSmem& sm, uint32_t x,
                                                     int* elem);
+__device__ __forceinline__ uint64_t torus_orbit_min(const GroupArgs& g, const GroupSmem& sm, uint64_t t,
+                                                    int* elem);
 
 // True iff no element maps s below s (s is its orbit's minimum).
 __device__ __forceinline__ bool is_rep(const GroupArgs& g, const GroupSmem& sm, uint64_t s) {
     if (g.full_rot) {
         int e;
         return chain_orbit_min(g, sm, (uint32_t)s, &e) == (uint32_t)s;
+    }
+    if (g.full_torus) {
+        int e;
+        return torus_orbit_min(g, sm, s, &e) == s;
     }
     if (g.structured && g.L <= 32) {
         const uint32_t x = (uint32_t)s, m = (uint32_t)g.mask;
@@ -214,10 +243,67 @@ __device__ __forceinline__ uint32_t chain_orbit_min(const GroupArgs& g, const Gr
     return best;
 }
 
+// The orbit minimum of t under all R x W translations of a torus of W-site
+// rows (and, with flip, their complements), and the first element reaching
+// it in the (element, inversion) order of orbit_min's loop.  The image of
+// translation (a rows, c sites) has as its top row (the most significant W
+// bits) row R-1-a of the string rotated by c, so the minimum's top row is the
+// smallest rotation of any row: only the translations that bring such a row,
+// rotated to that value, to the top are tried (usually a few of the R W, or
+// 2 R W with flip).
+__device__ __forceinline__ uint64_t torus_orbit_min(const GroupArgs& g, const GroupSmem& sm, uint64_t t,
+                                                    int* elem) {
+    const int W = g.W, R = g.L / g.W;
+    const uint64_t wmask = (1ull << W) - 1;
+    const int nz = g.n_ext > g.G ? 2 : 1;
+    int top[2] = {1 << 30, 1 << 30};
+    unsigned rows[2] = {0u, 0u};
+    for (int z = 0; z < nz; ++z) {
+        const uint64_t v = z ? (~t & g.mask) : t;
+        for (int i = 0; i < R; ++i) {
+            const int m = sm.minrot[(v >> (i * W)) & wmask];
+            if (m < top[z]) {
+                top[z] = m;
+                rows[z] = 1u << i;
+            } else if (m == top[z]) {
+                rows[z] |= 1u << i;
+            }
+        }
+    }
+    const int best_top = min(top[0], top[1]);
+    uint64_t best = t;  // element 0, the identity
+    int bg = 0, bz = 0;
+    for (int z = 0; z < nz; ++z) {
+        if (top[z] != best_top) continue;
+        const uint64_t v = z ? (~t & g.mask) : t;
+        unsigned rw = rows[z];
+        while (rw) {
+            const int i = __ffs(rw) - 1;
+            rw &= rw - 1;
+            const int a = R - 1 - i;  // row i moves to the top
+            unsigned cm = sm.rotmask[(v >> (i * W)) & wmask];
+            while (cm) {
+                const int c = __ffs(cm) - 1;
+                cm &= cm - 1;
+                const int gi = sm.gofr[a * W + c];
+                const uint64_t y = apply_site_map(g, sm, gi, v);
+                if (y < best || (y == best && (gi < bg || (gi == bg && z < bz)))) {
+                    best = y;
+                    bg = gi;
+                    bz = z;
+                }
+            }
+        }
+    }
+    *elem = bz ? bg + g.G : bg;
+    return best;
+}
+
 // Minimum of the orbit of t and the first element reaching it.
 __device__ __forceinline__ uint64_t orbit_min(const GroupArgs& g, const GroupSmem& sm, uint64_t t,
                                               int* elem) {
     if (g.full_rot) return chain_orbit_min(g, sm, (uint32_t)t, elem);
+    if (g.full_torus) return torus_orbit_min(g, sm, t, elem);
     if (g.structured && g.L <= 32) {
         const uint32_t x = (uint32_t)t, m = (uint32_t)g.mask;
         const bool flip = g.n_ext > g.G;

@@ -14,6 +14,7 @@ struct qmb_sector_s {
     // group on device
     int structured = 0, W = 0, n_chunks = 0;
     int full_rot = 0;  // a chain group of all L <= 32 rotations, element 0 the identity
+    int full_torus = 0;  // all translations of a torus of W <= 8 site rows, element 0 the identity
     qmb::DevBuf<qmb::ElemRot> rot;
     qmb::DevBuf<uint64_t> tables;
 
@@ -43,6 +44,7 @@ struct qmb_sector_s {
         g.W = W;
         g.n_chunks = n_chunks;
         g.full_rot = full_rot;
+        g.full_torus = full_torus;
         g.mask = (L == 64) ? ~0ull : ((1ull << L) - 1);
         g.rot = rot.p;
         g.tables = tables.p;

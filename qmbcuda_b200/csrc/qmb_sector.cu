@@ -298,9 +298,9 @@ void sector_setup(qmb_sector_s* s, const qmb_sector_desc* d) {
         for (int g = 0; g < G; ++g) distinct = distinct && !seen[rots[g].ri]++;
         s->full_rot = distinct ? 1 : 0;
     }
-    // all R x W translations of a torus of W <= 8 site rows, element 0 the identity
+    // all R x W translations of a torus of W <= 8 site rows (R <= 32), element 0 the identity
     s->full_torus = 0;
-    if (structured && s->W < L && s->W <= 8 && G == L && rots[0].ri == 0 && rots[0].rr == 0) {
+    if (structured && s->W < L && s->W <= 8 && L / s->W <= 32 && G == L && rots[0].ri == 0 && rots[0].rr == 0) {
         std::vector<int> seen(L, 0);
         bool distinct = true;
         for (int g = 0; g < G; ++g) {

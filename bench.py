@@ -868,9 +868,9 @@ def main():
     ap.add_argument("--profile-k1", action="store_true",
                     help="build the L=20 batch and time 5 FP32 Lanczos-step products (K1), then exit "
                          "(the launches the K1 ncu summary profiles)")
-    ap.add_argument("--profile-matrix-free", action="store_true",
-                    help="two matrix-free FP32 products on the L=32 J1-J2 k=0 even sector, then exit "
-                         "(the launch the matrix-free ncu summary profiles)")
+    ap.add_argument("--profile-matrix-free", nargs="?", const="l32", choices=["l32", "6x6"], default=None,
+                    help="matrix-free FP32 products on the L=32 J1-J2 k=0 even sector (default) or the 6x6 "
+                         "k=(0,0) even sector, then exit (the launches the matrix-free ncu summaries profile)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -936,11 +936,20 @@ def main():
 
     if args.profile_matrix_free:
         A = q._capi
-        L = 32
-        perm, ch = q.translation_group(L)
-        s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
-        J = [1.0] * L + [0.5] * L
-        h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J), prec=A.PREC_FP32)
+        if args.profile_matrix_free == "6x6":
+            N = 6
+            perm, ch = q.translation_group(N, N)
+            s = q.Sector(N * N, N * N // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+            terms = q.xxz_terms(q.square_bonds(N, N), 1.0, 1.0)
+            name = "6x6 square k=(0,0) even"
+        else:
+            L = 32
+            perm, ch = q.translation_group(L)
+            s = q.Sector(L, L // 2, perm, spin_flip=True).set_irrep(q.with_spin_flip(ch[0], 1))
+            J = [1.0] * L + [0.5] * L
+            terms = q.xxz_terms(q.chain_bonds(L) + q.chain_bonds(L, 2), J, J)
+            name = "L=32 J1-J2 k=0 even"
+        h = q.Hamiltonian(s, terms, prec=A.PREC_FP32)
         x = torch.randn(int(h.info.n_rows), dtype=torch.float32, device="cuda")
         y = torch.empty_like(x)
         args_mf = (h.h, A.PREC_FP32, A.C.c_void_p(x.data_ptr()), A.C.c_void_p(y.data_ptr()), None)
@@ -953,8 +962,8 @@ def main():
             q.check(q.lib().qmb_hv_matrix_free(*args_mf))
         e1.record()
         e1.synchronize()
-        print(json.dumps({"profile": "matrix-free FP32 product, L=32 J1-J2 k=0 even", "rows": int(h.info.n_rows),
-                          "ms": e0.elapsed_time(e1) / 3}))
+        print(json.dumps({"profile": f"matrix-free FP32 product, {name}", "rows": int(h.info.n_rows),
+                          "nnz": int(h.info.nnz_offdiag), "ms": e0.elapsed_time(e1) / 3}))
         return 0
 
     if args.hv_only:

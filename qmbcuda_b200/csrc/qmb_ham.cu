@@ -613,6 +613,26 @@ __global__ void k_mf_bucket(const K* __restrict__ reps, int64_t n, int shift, ui
     }
 }
 
+// Fills the matrix-free hash table: row i under its representative.
+__global__ void k_mf_hash(const uint64_t* __restrict__ reps, int64_t n, uint64_t* __restrict__ tab, uint64_t mask,
+                          int hidx) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = reps[i];
+        const uint64_t w = (r << hidx) | (uint64_t)i;
+        uint64_t slot = mf_hash_slot(r, mask);
+        for (uint64_t it = 0; it <= mask; ++it) {  // the table is at most half full
+            const unsigned long long prev =
+                atomicCAS(reinterpret_cast<unsigned long long*>(tab + slot), kMfHashEmpty, (unsigned long long)w);
+            if (prev == kMfHashEmpty) break;
+            slot = (slot + 1) & mask;
+        }
+    }
+}
+
+// Representative tables at least this large (beyond 32 sites) also get the
+// hash table: four times what stays comfortably in the 126 MB L2.
+constexpr double kMfHashMinBytes = 512.0 * 1024 * 1024;
+
 // The stored diagonal of the hop form.
 template <class D>
 __global__ void k_mf_diag(RowGen rg, int64_t n, D* __restrict__ diag) {
@@ -655,6 +675,21 @@ void mf_tables(qmb_ham_s* h) {
     else k_mf_bucket<uint64_t><<<g, 256>>>(all ? s->reps.p : h->mf_reps64.p, n, h->mf_shift, h->mf_nb,
                                               h->mf_bucket.p);
     check_launch("k_mf_bucket");
+    // beyond 32 sites with a representative table well beyond L2: the hash
+    // table, when a representative and a row index fit one word (top bit 0)
+    int ibits = 1;
+    while (ibits < 63 && ((n - 1) >> ibits)) ++ibits;
+    if (!r32 && (double)n * 8 >= kMfHashMinBytes && bits + ibits <= 63) {
+        uint64_t slots = 1;
+        while (slots < 2 * (uint64_t)n) slots <<= 1;
+        h->mf_hash.alloc(slots);
+        QMB_CUDA_TRY(cudaMemset(h->mf_hash.p, 0xff, slots * sizeof(uint64_t)));
+        h->mf_hmask = slots - 1;
+        h->mf_hidx = ibits;
+        k_mf_hash<<<grid_for(n, 256), 256>>>(all ? s->reps.p : h->mf_reps64.p, n, h->mf_hash.p, h->mf_hmask,
+                                             ibits);
+        check_launch("k_mf_hash");
+    }
     if (h->n_hops) {
         const RowGen rg = h->row_gen();
         const size_t sm = gen_smem(rg);

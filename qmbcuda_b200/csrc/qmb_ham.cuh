@@ -1,5 +1,7 @@
 // qmb_ham.cuh -- Hamiltonian storage and the row operators used by H*v.
 #pragma once
+#include <cstdlib>
+
 #include "qmb_scalar.cuh"
 #include "qmb_sector.cuh"
 
@@ -356,6 +358,15 @@ struct RefEllOp {
 // their top bits, so a generated representative maps straight to its row.
 // The norm factor is left out (f = 1): the operator gathers n(c) x_c and
 // divides the row by its own norm.
+// Slot of a representative in the matrix-free hash table: the splitmix64
+// finaliser (Steele, Lea and Flood 2014) of the representative.
+__host__ __device__ __forceinline__ uint64_t mf_hash_slot(uint64_t r, uint64_t mask) {
+    r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ull;
+    r = (r ^ (r >> 27)) * 0x94D049BB133111EBull;
+    return (r ^ (r >> 31)) & mask;
+}
+constexpr uint64_t kMfHashEmpty = ~0ull;
+
 struct ActiveLookup {
     const uint32_t* reps32;  // [n] or null
     const uint64_t* reps64;  // [n] when reps32 is null
@@ -364,7 +375,30 @@ struct ActiveLookup {
     uint64_t n_b;
     int64_t n;
     int all_active;          // every orbit is a row: a miss is outside the sector
+    // Open-addressing table (linear probing, at most half full) of the rows
+    // of a sector whose representative table is larger than L2: one 64-bit
+    // word per row, (representative << hidx) | row, kMfHashEmpty when free.
+    // A lookup then reads one word (usually one 32-byte sector) instead of a
+    // bucket entry and a binary search over 8-byte representatives.
+    const uint64_t* hash;    // [hmask + 1] or null
+    uint64_t hmask;
+    int hidx;                // bits of the row index in a word
     __device__ __forceinline__ int find(const RowGen& rg, uint64_t r, int64_t* idx, double* f) const {
+        if (hash) {
+            uint64_t slot = mf_hash_slot(r, hmask);
+            for (uint64_t it = 0; it <= hmask; ++it) {
+                const uint64_t w = __ldg(hash + slot);
+                if (w == kMfHashEmpty) break;
+                if ((w >> hidx) == r) {
+                    *idx = (int64_t)(w & ((1ull << hidx) - 1));
+                    *f = 1.0;
+                    return 1;
+                }
+                slot = (slot + 1) & hmask;
+            }
+            if (all_active) return -1;
+            return find_rep(rg.rt, r) < 0 ? -1 : 0;  // a null orbit, or outside the sector
+        }
         const uint64_t b = r >> shift;
         int64_t lo = 0, hi = 0;
         if (b < n_b) {
@@ -675,6 +709,9 @@ struct qmb_ham_s {
     qmb::DevBuf<uint32_t> mf_reps32;   // [n] active representatives, L <= 32
     qmb::DevBuf<uint64_t> mf_reps64;   // [n] L > 32 with null orbits (else the sector's table)
     qmb::DevBuf<uint32_t> mf_bucket;   // [mf_nb + 1]
+    qmb::DevBuf<uint64_t> mf_hash;     // rows by representative, beyond 32 sites when the table exceeds L2
+    uint64_t mf_hmask = 0;
+    int mf_hidx = 0;
     qmb::DevBuf<double> mf_norm;       // [n] norm of each row's orbit
     qmb::DevBuf<unsigned char> mf_diag;  // [n] diagonal with a hop table (double2 if complex)
     qmb::DevBuf<unsigned char> mf_xs;  // [n] n(c) x_c in the product's vector type
@@ -748,6 +785,11 @@ struct qmb_ham_s {
         op.look.n_b = mf_nb;
         op.look.n = n;
         op.look.all_active = sector->n_active == sector->R ? 1 : 0;
+        // QMB_MF_HASH=0 searches the bucket table even where the hash table exists
+        const char* he = std::getenv("QMB_MF_HASH");
+        op.look.hash = (mf_hash.p && !(he && he[0] == '0')) ? mf_hash.p : nullptr;
+        op.look.hmask = mf_hmask;
+        op.look.hidx = mf_hidx;
         op.nrow = mf_norm.p;
         op.xs = mf_xs.p;
         op.n_hops = n_hops;

@@ -64,7 +64,11 @@ def test_l32_j1j2_matrix_free_and_fp32_reorth():
     assert rmx.residual < 1e-6
 
 
-def test_6x6_k0_even_sector_and_hermitian_hv():
+def test_6x6_k0_even_sector_and_hermitian_hv(monkeypatch):
+    """The 6x6 k=(0,0) even sector (126 M rows): the stored and matrix-free
+    FP32 products agree and are Hermitian; the matrix-free product looks its
+    rows up in the hash table (the representative table is 1 GB) and gives
+    the same bits as with the bucket search (QMB_MF_HASH=0)."""
     import torch
     N = 6
     perm, ch = q.translation_group(N, N)
@@ -81,7 +85,12 @@ def test_6x6_k0_even_sector_and_hermitian_hv():
     _stored(h, A.PREC_FP32, x, hx)
     _stored(h, A.PREC_FP32, z, hz)
     _mf(h, A.PREC_FP32, x, hx2)
+    monkeypatch.setenv("QMB_MF_HASH", "0")
+    hx3 = torch.empty_like(x)
+    _mf(h, A.PREC_FP32, x, hx3)
+    monkeypatch.delenv("QMB_MF_HASH")
     torch.cuda.synchronize()
+    assert torch.equal(hx2, hx3)
     assert float((hx - hx2).abs().max()) <= 1e-4 * float(hx.abs().max())
     a = float(torch.dot(z.double(), hx.double()))
     b = float(torch.dot(hz.double(), x.double()))

@@ -209,6 +209,24 @@ __global__ void __launch_bounds__(256, OpMinBlocks<Op>::value) k_hv(Op op, const
     }
 }
 
+// The matrix-free product with the warp-cooperative lookup (hop form): the
+// rows run a warp at a time, so that every lane takes part in the warp's
+// lookups, including lanes past the last row.
+template <class M, class V>
+__global__ void __launch_bounds__(256, 5) k_hv_mfw(MfOp<M> op, const V* __restrict__ x, V* __restrict__ y) {
+    extern __shared__ __align__(16) unsigned char smem_hv[];
+    op.init(smem_hv);
+    const int lane = threadIdx.x & 31;
+    for (int64_t r0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - lane; r0 < op.n;
+         r0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = r0 + lane;
+        const bool act = r < op.n;
+        V xr;
+        const V v = op.template row_warp<V>(act, act ? r : r0, x, xr);
+        if (act) y[r] = v;
+    }
+}
+
 template <class M32, class M64>
 __global__ void k_narrow(const M64* __restrict__ a, M32* __restrict__ b, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -840,6 +858,28 @@ void hv_dispatch(const qmb_ham_s* h, int prec, const void* x, void* y, cudaStrea
     QMB_REQUIRE(prec == QMB_PREC_FP64 || prec == QMB_PREC_FP32, QMB_ERR_INVALID,
                 "prec must be QMB_PREC_FP64 or QMB_PREC_FP32");
     if (matrix_free) {
+        // QMB_MF_LOOKUP=warp: the warp-cooperative lookup over the bucket table
+        const char* le = std::getenv("QMB_MF_LOOKUP");
+        if (le && std::strcmp(le, "warp") == 0 && h->n_hops) {
+            auto run = [&](auto op, auto* xv, auto* yv) {
+                using V = std::remove_const_t<std::remove_pointer_t<decltype(xv)>>;
+                using MT = typename decltype(op)::scalar;
+                op.look.hash = nullptr;
+                const size_t sm = op.smem_bytes();
+                set_group_smem_attr((const void*)k_hv_mfw<MT, V>, sm);
+                op.pre(xv, (const int*)nullptr, st);
+                k_hv_mfw<MT, V><<<grid_for(op.n, 256), 256, sm, st>>>(op, xv, yv);
+                check_launch("k_hv_mfw");
+            };
+            if (h->cplx) {
+                if (f64) run(h->mf<double2>(), (const double2*)x, (double2*)y);
+                else run(h->mf<float2>(), (const float2*)x, (float2*)y);
+            } else {
+                if (f64) run(h->mf<double>(), (const double*)x, (double*)y);
+                else run(h->mf<float>(), (const float*)x, (float*)y);
+            }
+            return;
+        }
         if (h->cplx) {
             if (f64) { auto op = h->mf<double2>(); launch_hv(op, (const double2*)x, (double2*)y, st, op.smem_bytes()); }
             else { auto op = h->mf<float2>(); launch_hv(op, (const float2*)x, (float2*)y, st, op.smem_bytes()); }

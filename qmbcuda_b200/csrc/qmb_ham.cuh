@@ -430,6 +430,51 @@ struct ActiveLookup {
         if (all_active) return -1;
         return find_rep(rg.rt, r) < 0 ? -1 : 0;  // a null orbit, or outside the sector
     }
+    // Warp-cooperative form of find() over the bucket table: the 32 lanes of a
+    // warp call it together (has = false for a lane without a target).  The
+    // lanes' targets are taken one at a time; for each, the warp compares 32
+    // consecutive representatives of its bucket range in one coalesced load
+    // and a ballot gives the position (ranges longer than 32 take more
+    // rounds).  A binary search makes log2(range) dependent loads per lane
+    // instead, each from its own line.
+    __device__ __forceinline__ int find_warp(const RowGen& rg, bool has, uint64_t r, int64_t* idx,
+                                             double* f) const {
+        const int lane = threadIdx.x & 31;
+        int64_t lo = 0, hi = 0;
+        if (has) {
+            const uint64_t b = r >> shift;
+            if (b < n_b) {
+                lo = bucket[b];
+                hi = bucket[b + 1];
+            }
+        }
+        int64_t pos = -1;
+        unsigned pend = __ballot_sync(0xffffffffu, has && lo < hi);
+        while (pend) {
+            const int t = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t rt = __shfl_sync(0xffffffffu, r, t);
+            const int64_t lt = __shfl_sync(0xffffffffu, lo, t), ht = __shfl_sync(0xffffffffu, hi, t);
+            for (int64_t base = lt; base < ht; base += 32) {
+                const int64_t p = base + lane;
+                bool eq = false;
+                if (p < ht) eq = (reps32 ? (uint64_t)__ldg(reps32 + p) : __ldg(reps64 + p)) == rt;
+                const unsigned m = __ballot_sync(0xffffffffu, eq);
+                if (m) {
+                    if (lane == t) pos = base + __ffs(m) - 1;
+                    break;
+                }
+            }
+        }
+        if (!has) return 0;
+        if (pos >= 0) {
+            *idx = pos;
+            *f = 1.0;
+            return 1;
+        }
+        if (all_active) return -1;
+        return find_rep(rg.rt, r) < 0 ? -1 : 0;  // a null orbit, or outside the sector
+    }
     // find() of two representatives at once for L <= 32 (reps32 set), in
     // 32-bit arithmetic: the two searches run in
     // lockstep, so each step has two independent loads in flight
@@ -502,6 +547,7 @@ struct CbLayout {
 // 32 sites the strings, masks, representatives and row indices are 32-bit.
 template <class M>
 struct MfOp {
+    using scalar = M;
     int64_t n;
     RowGen rg;
     ActiveLookup look;
@@ -624,6 +670,57 @@ struct MfOp {
             }
         }
         return acc;
+    }
+    // The hop sum with the warp-cooperative lookup: the 32 lanes (rows) of a
+    // warp step through their live hops together, one hop a lane a round,
+    // until every lane's hops are done (act = false: a lane without a row).
+    template <class V>
+    __device__ __forceinline__ V hop_sum_warp(bool act, uint64_t src, const V* __restrict__ xsv) const {
+        V acc = Sc<V>::zero();
+        for (int base = 0; base < n_hops; base += 64) {
+            const int nb = min(64, n_hops - base);
+            uint64_t live = 0;
+            if (act)
+                for (int b = 0; b < nb; ++b) live |= (uint64_t)(__popcll(src & s_hops[base + b].pair) & 1) << b;
+            while (__any_sync(0xffffffffu, live != 0)) {
+                bool has = live != 0;
+                double2 cf = make_double2(0.0, 0.0);
+                uint64_t rr = 0;
+                int e = 0;
+                if (has) {
+                    const int b = base + __ffsll((long long)live) - 1;
+                    live &= live - 1;
+                    const uint64_t pair = s_hops[b].pair;
+                    cf = s_hop_c[2 * b + ((src & pair & (0ull - pair)) ? 1 : 0)];
+                    if (hop_one_way && cf.x == 0.0 && cf.y == 0.0) has = false;  // no term in this direction
+                    else rr = orbit_min(rg.g, gs, src ^ pair, &e);
+                }
+                int64_t c = 0;
+                double f;
+                const int found = look.find_warp(rg, has, rr, &c, &f);
+                if (has && found < 0) *rg.err = 2;
+                if (has && found > 0) {
+                    const double2 ch = rg.g.chars[e];
+                    const double2 v = make_double2(cf.x * ch.x + cf.y * ch.y, cf.y * ch.x - cf.x * ch.y);
+                    acc = Sc<V>::fma(Sc<V>::from(v), __ldg(xsv + c), acc);
+                }
+            }
+        }
+        return acc;
+    }
+    // row() with the warp-cooperative lookup (hop form only); every lane of
+    // the warp calls it, act = false where the lane has no row (r is then any
+    // valid row and the result is not used)
+    template <class V>
+    __device__ __forceinline__ V row_warp(bool act, int64_t r, const V* __restrict__ x, V& xr) const {
+        const uint64_t rep = look.reps32 ? (uint64_t)look.reps32[r] : look.reps64[r];
+        const uint64_t src = apply_elem(rg.g, gs, 0, rep);
+        xr = x[r];
+        V acc = hop_sum_warp<V>(act, src, reinterpret_cast<const V*>(xs));
+        const double2 d = cplx ? reinterpret_cast<const double2*>(diag)[r]
+                               : make_double2(reinterpret_cast<const double*>(diag)[r], 0.0);
+        acc = Sc<V>::scale(acc, 1.0 / nrow[r]);
+        return Sc<V>::fma(Sc<V>::from(d), xr, acc);
     }
     template <class V>
     __device__ __forceinline__ V row(int64_t r, const V* __restrict__ x, V& xr) const {

@@ -151,13 +151,14 @@ def test_hv_stored_and_matrix_free(case):
                                          (32, 4, False, 0), (32, 4, False, 1), (36, 3, False, 0),
                                          (36, 3, False, 1), (34, 4, False, 11)],
                          ids=lambda v: str(v))
-def test_matrix_free_active_lookup(L, k, flip, a):
+def test_matrix_free_active_lookup(L, k, flip, a, monkeypatch):
     """The matrix-free operator's row lookup over the active orbits: 32-bit
     representatives up to L = 32 (the run-candidate orbit minimum of full
     rotation groups, funnel shifts at L = 32), 64-bit beyond; the sector's
     tables when every orbit is active, its own bucket table when some orbits
-    are null.  FP64 and FP32 products against the oracle's matrix, and a
-    matrix-free FP64 solve against the stored one."""
+    are null.  FP64 and FP32 products against the oracle's matrix, with the
+    per-lane search and with the warp-cooperative one (QMB_MF_LOOKUP=warp),
+    and a matrix-free FP64 solve against the stored one."""
     import torch
     perm, ch = q.translation_group(L)
     chars = np.block([[ch, ch], [ch, -ch]]) if flip else ch
@@ -176,16 +177,19 @@ def test_matrix_free_active_lookup(L, k, flip, a):
     rng = np.random.default_rng(L + a)
     x = rng.standard_normal(n) + (1j * rng.standard_normal(n) if h.info.is_complex else 0)
     y_o = A @ x
-    for prec, tol in ((q._capi.PREC_FP64, 1e-12), (q._capi.PREC_FP32, 2e-6)):
-        if prec == q._capi.PREC_FP64:
-            dt = torch.complex128 if h.info.is_complex else torch.float64
-        else:
-            dt = torch.complex64 if h.info.is_complex else torch.float32
-        xd = torch.tensor(x, dtype=dt, device="cuda")
-        yd = torch.zeros_like(xd)
-        h.hv_dev(xd.data_ptr(), yd.data_ptr(), prec, matrix_free=True)
-        torch.cuda.synchronize()
-        np.testing.assert_allclose(yd.cpu().numpy(), y_o, rtol=0, atol=tol * np.abs(y_o).max())
+    for lookup in ("lane", "warp"):
+        monkeypatch.setenv("QMB_MF_LOOKUP", lookup)
+        for prec, tol in ((q._capi.PREC_FP64, 1e-12), (q._capi.PREC_FP32, 2e-6)):
+            if prec == q._capi.PREC_FP64:
+                dt = torch.complex128 if h.info.is_complex else torch.float64
+            else:
+                dt = torch.complex64 if h.info.is_complex else torch.float32
+            xd = torch.tensor(x, dtype=dt, device="cuda")
+            yd = torch.zeros_like(xd)
+            h.hv_dev(xd.data_ptr(), yd.data_ptr(), prec, matrix_free=True)
+            torch.cuda.synchronize()
+            np.testing.assert_allclose(yd.cpu().numpy(), y_o, rtol=0, atol=tol * np.abs(y_o).max())
+    monkeypatch.delenv("QMB_MF_LOOKUP")
     A64 = q._capi
     r_st = h.lanczos(mode=A64.MODE_FP64, tol=1e-12)
     r_mf = h.lanczos(mode=A64.MODE_FP64, tol=1e-12, hv=A64.HV_MATRIX_FREE)

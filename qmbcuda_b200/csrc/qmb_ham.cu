@@ -694,10 +694,13 @@ void mf_tables(qmb_ham_s* h) {
                                               h->mf_bucket.p);
     check_launch("k_mf_bucket");
     // beyond 32 sites with a representative table well beyond L2: the hash
-    // table, when a representative and a row index fit one word (top bit 0)
+    // table, when a representative and a row index fit one word (top bit 0);
+    // QMB_MF_HASH=1 builds it at any size (tests)
     int ibits = 1;
     while (ibits < 63 && ((n - 1) >> ibits)) ++ibits;
-    if (!r32 && (double)n * 8 >= kMfHashMinBytes && bits + ibits <= 63) {
+    const char* he = std::getenv("QMB_MF_HASH");
+    const bool force_hash = he && he[0] == '1';
+    if (!r32 && (force_hash || (double)n * 8 >= kMfHashMinBytes) && bits + ibits <= 63) {
         uint64_t slots = 1;
         while (slots < 2 * (uint64_t)n) slots <<= 1;
         h->mf_hash.alloc(slots);

@@ -156,9 +156,11 @@ def test_matrix_free_active_lookup(L, k, flip, a, monkeypatch):
     representatives up to L = 32 (the run-candidate orbit minimum of full
     rotation groups, funnel shifts at L = 32), 64-bit beyond; the sector's
     tables when every orbit is active, its own bucket table when some orbits
-    are null.  FP64 and FP32 products against the oracle's matrix, with the
-    per-lane search and with the warp-cooperative one (QMB_MF_LOOKUP=warp),
-    and a matrix-free FP64 solve against the stored one."""
+    are null; beyond 32 sites the hash table as well (forced here with
+    QMB_MF_HASH=1, including its misses on null orbits).  FP64 and FP32
+    products against the oracle's matrix with each lookup (per-lane hash,
+    per-lane bucket search, warp-cooperative), and a matrix-free FP64 solve
+    against the stored one."""
     import torch
     perm, ch = q.translation_group(L)
     chars = np.block([[ch, ch], [ch, -ch]]) if flip else ch
@@ -177,8 +179,12 @@ def test_matrix_free_active_lookup(L, k, flip, a, monkeypatch):
     rng = np.random.default_rng(L + a)
     x = rng.standard_normal(n) + (1j * rng.standard_normal(n) if h.info.is_complex else 0)
     y_o = A @ x
-    for lookup in ("lane", "warp"):
+    # beyond 32 sites the handle also gets the hash table (forced at this
+    # size), searched by default; QMB_MF_HASH=0 searches the bucket table
+    monkeypatch.setenv("QMB_MF_HASH", "1")
+    for lookup, hash_env in (("lane", "1"), ("lane", "0"), ("warp", "1")):
         monkeypatch.setenv("QMB_MF_LOOKUP", lookup)
+        monkeypatch.setenv("QMB_MF_HASH", hash_env)
         for prec, tol in ((q._capi.PREC_FP64, 1e-12), (q._capi.PREC_FP32, 2e-6)):
             if prec == q._capi.PREC_FP64:
                 dt = torch.complex128 if h.info.is_complex else torch.float64
@@ -190,6 +196,7 @@ def test_matrix_free_active_lookup(L, k, flip, a, monkeypatch):
             torch.cuda.synchronize()
             np.testing.assert_allclose(yd.cpu().numpy(), y_o, rtol=0, atol=tol * np.abs(y_o).max())
     monkeypatch.delenv("QMB_MF_LOOKUP")
+    monkeypatch.delenv("QMB_MF_HASH")
     A64 = q._capi
     r_st = h.lanczos(mode=A64.MODE_FP64, tol=1e-12)
     r_mf = h.lanczos(mode=A64.MODE_FP64, tol=1e-12, hv=A64.HV_MATRIX_FREE)

@@ -286,7 +286,10 @@ typedef struct {
     int max_iter;       /* Krylov steps of the (first) phase; fixed count when tol <= 0 */
     int min_iter;
     double tol;         /* relative: stop when residual estimate < tol*|E| and dE < tol*|E| */
-    int reorth;         /* 1: full reorthogonalization (two classical Gram-Schmidt passes) */
+    int reorth;         /* full reorthogonalization against the stored basis: classical
+                           Gram-Schmidt passes a step, 0..2; the second pass runs when
+                           the first removed more than 1 - 1/sqrt(2) of the vector's
+                           norm (Kahan-Parlett), every step with QMB_REORTH_ALWAYS=1 */
     int start;          /* QMB_START_* */
     uint64_t seed;
     int check_every;    /* convergence test interval (iterations) */

@@ -155,15 +155,29 @@ __global__ void __launch_bounds__(kLzBlock) k_lz_update(int64_t n, V* __restrict
     }
 }
 
-// Reorthogonalisation, pass 1: coefs[i] = <v_i, w_{j+1}> for i <= j, eight
-// basis vectors a sweep over the rows (w is read once per eight).
+// Classical Gram-Schmidt with the Kahan-Parlett criterion ("twice is
+// enough", as in the DGKS correction): with two passes requested, the second
+// pass runs only when the first removed enough of w that its rounding can
+// matter, ||w'|| < kReorthEta ||w||.  scratch[2] keeps ||w|| before the first
+// pass and scratch[3] is 1 when the second pass must run.
+constexpr double kReorthEta = 0.70710678118654752;
+
+// Reorthogonalisation, dot half of a pass: coefs[i] = <v_i, w_{j+1}> for
+// i <= j, eight basis vectors a sweep over the rows (w is read once per
+// eight).  Pass 0 records ||w|| first; pass 1 returns at once when the first
+// pass made it unnecessary.
 constexpr int kDotChunk = 8;
 template <class V>
 __global__ void __launch_bounds__(kLzBlock) k_reorth_dots(int64_t n, const V* __restrict__ wbuf,
-                                                          const V* __restrict__ vring, LzDev d) {
+                                                          const V* __restrict__ vring, LzDev d, int pass) {
     __shared__ double red[2 * kDotChunk * (kLzBlock / 32)];
     __shared__ bool last;
     const int j = *d.iter;
+    if (pass == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) d.scratch[2] = d.beta[j + 1];
+    } else if (d.scratch[3] == 0.0) {
+        return;
+    }
     const V* Y = wbuf + (int64_t)((j + 1) & 1) * n;
     const int nb = gridDim.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
@@ -232,15 +246,21 @@ __global__ void __launch_bounds__(kLzBlock) k_reorth_dots(int64_t n, const V* __
     if (threadIdx.x == 0) *d.counter = 0;
 }
 
-// Reorthogonalisation, pass 2: w_{j+1} -= sum_i coefs[i] v_i; beta_{j+1} = ||w_{j+1}||.
+// Reorthogonalisation, update half of a pass: w_{j+1} -= sum_i coefs[i] v_i;
+// beta_{j+1} = ||w_{j+1}||.  After pass 0, scratch[3] says whether pass 1
+// runs (always when `selective` is 0); a skipped pass 1 only finalizes.
 template <class V>
 __global__ void __launch_bounds__(kLzBlock) k_reorth_update(int64_t n, V* __restrict__ wbuf,
                                                             const V* __restrict__ vring, LzDev d,
-                                                            int finalize) {
+                                                            int finalize, int pass, int selective) {
     extern __shared__ __align__(16) unsigned char smem_ro[];
     __shared__ double red[32];
     double2* cf = reinterpret_cast<double2*>(smem_ro);
     const int j = *d.iter;
+    if (pass == 1 && d.scratch[3] == 0.0) {
+        if (finalize && blockIdx.x == 0 && threadIdx.x == 0) *d.iter = j + 1;
+        return;
+    }
     for (int i = threadIdx.x; i <= j; i += blockDim.x) cf[i] = d.coefs[i];
     __syncthreads();
     V* Y = wbuf + (int64_t)((j + 1) & 1) * n;
@@ -257,7 +277,9 @@ __global__ void __launch_bounds__(kLzBlock) k_reorth_update(int64_t n, V* __rest
     }
     double tot;
     if (grid_reduce(acc, d.partials, d.counter, red, &tot) && threadIdx.x == 0) {
-        d.beta[j + 1] = sqrt(tot);
+        const double b = sqrt(tot);
+        d.beta[j + 1] = b;
+        if (pass == 0) d.scratch[3] = (!selective || b < kReorthEta * d.scratch[2]) ? 1.0 : 0.0;
         if (finalize) *d.iter = j + 1;
     }
 }
@@ -299,6 +321,13 @@ __global__ void k_residual(Op op, const P* __restrict__ psi, double theta, LzDev
 }
 
 // ------------------------------------------------------------------- host
+// QMB_REORTH_ALWAYS=1: with two passes requested, always run the second one
+// (by default it runs only when the Kahan-Parlett criterion asks for it).
+static bool reorth_selective() {
+    const char* e = std::getenv("QMB_REORTH_ALWAYS");
+    return !(e && e[0] == '1');
+}
+
 static int lz_ring_max() {
     const char* e = std::getenv("QMB_LZ_RING_MAX");
     return e ? std::max(0, std::atoi(e)) : 0;
@@ -326,6 +355,7 @@ struct LzState {
         beta.alloc(cap + 2);
         partials.alloc(2 * (size_t)nb);
         scratch.alloc(4);
+        scratch.zero();
         iter.alloc(1);
         counter.alloc(2);
         counter.zero();
@@ -460,9 +490,10 @@ PhaseOut run_phase(const Op& op, size_t op_smem, const PhaseOpts& po, int start_
                                                          (P*)nullptr);
         k_lz_update<V><<<nb, kLzBlock, 0, ss>>>(n, wbuf.p, vring.p, K, st.d, po.reorth ? 0 : 1);
         for (int p = 0; p < po.reorth; ++p) {
-            k_reorth_dots<V><<<nb, kLzBlock, 0, ss>>>(n, wbuf.p, vring.p, st.d);
+            k_reorth_dots<V><<<nb, kLzBlock, 0, ss>>>(n, wbuf.p, vring.p, st.d, p);
             k_reorth_update<V><<<nb, kLzBlock, ro_smem, ss>>>(n, wbuf.p, vring.p, st.d,
-                                                              p == po.reorth - 1 ? 1 : 0);
+                                                              p == po.reorth - 1 ? 1 : 0, p,
+                                                              reorth_selective() ? 1 : 0);
         }
     };
 

@@ -163,13 +163,14 @@ __global__ void __launch_bounds__(kLzBlock) k_lz_update(int64_t n, V* __restrict
 constexpr double kReorthEta = 0.70710678118654752;
 
 // Reorthogonalisation, dot half of a pass: coefs[i] = <v_i, w_{j+1}> for
-// i <= j, eight basis vectors a sweep over the rows (w is read once per
-// eight).  Pass 0 records ||w|| first; pass 1 returns at once when the first
-// pass made it unnecessary.
-constexpr int kDotChunk = 8;
+// i <= j, kDotChunk basis vectors a sweep over the rows (w is read once per
+// chunk): 16 for real and complex FP32 vectors, 8 for complex FP64.  Pass 0
+// records ||w|| first; pass 1 returns at once when the first pass made it
+// unnecessary.
 template <class V>
 __global__ void __launch_bounds__(kLzBlock) k_reorth_dots(int64_t n, const V* __restrict__ wbuf,
                                                           const V* __restrict__ vring, LzDev d, int pass) {
+    constexpr int kDotChunk = sizeof(V) >= 16 ? 8 : 16;
     __shared__ double red[2 * kDotChunk * (kLzBlock / 32)];
     __shared__ bool last;
     const int j = *d.iter;
@@ -268,10 +269,18 @@ __global__ void __launch_bounds__(kLzBlock) k_reorth_update(int64_t n, V* __rest
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
          r += (int64_t)gridDim.x * blockDim.x) {
         V y = Y[r];
-        for (int i = 0; i <= j; ++i) {
-            V v = vring[(int64_t)i * n + r];
-            y = Sc<V>::sub(y, Sc<V>::mul(Sc<V>::from(cf[i]), v));
+        // U basis rows loaded before their products are subtracted, so that
+        // U loads per thread are in flight instead of one
+        constexpr int U = sizeof(V) >= 16 ? 8 : 16;
+        int i = 0;
+        for (; i + U <= j + 1; i += U) {
+            V v[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) v[k] = vring[(int64_t)(i + k) * n + r];
+#pragma unroll
+            for (int k = 0; k < U; ++k) y = Sc<V>::sub(y, Sc<V>::mul(Sc<V>::from(cf[i + k]), v[k]));
         }
+        for (; i <= j; ++i) y = Sc<V>::sub(y, Sc<V>::mul(Sc<V>::from(cf[i]), vring[(int64_t)i * n + r]));
         Y[r] = y;
         acc += Sc<V>::abs2(y);
     }

@@ -300,8 +300,17 @@ __global__ void k_ritz(int64_t n, const V* __restrict__ vring, int m,
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
          r += (int64_t)gridDim.x * blockDim.x) {
         P acc = Sc<P>::zero();
-        for (int i = 0; i < m; ++i)
-            acc = Sc<P>::add(acc, Sc<P>::scale(cvt<P>(vring[(int64_t)i * n + r]), ritz[i]));
+        // U basis rows in flight a thread, summed in index order
+        constexpr int U = sizeof(V) >= 16 ? 8 : 16;
+        int i = 0;
+        for (; i + U <= m; i += U) {
+            V v[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) v[k] = vring[(int64_t)(i + k) * n + r];
+#pragma unroll
+            for (int k = 0; k < U; ++k) acc = Sc<P>::add(acc, Sc<P>::scale(cvt<P>(v[k]), ritz[i + k]));
+        }
+        for (; i < m; ++i) acc = Sc<P>::add(acc, Sc<P>::scale(cvt<P>(vring[(int64_t)i * n + r]), ritz[i]));
         psi[r] = acc;
     }
 }

@@ -78,6 +78,29 @@ def test_config1_l16_full_reorth_150_steps():
     assert r.residual < 1e-8
 
 
+def test_selective_second_reorthogonalisation_pass(monkeypatch):
+    """reorth=2 runs the second Gram-Schmidt pass only when the first removed
+    more than 1 - 1/sqrt(2) of the vector (Kahan-Parlett); QMB_REORTH_ALWAYS=1
+    runs it every step.  Same energy and residual level either way, FP64 and
+    mixed, on the 150-step L=16 solve and an L=14 momentum sector."""
+    L = 16
+    s = q.Sector(L, 8, np.arange(L, dtype=np.uint32)[None]).set_irrep([1.0])
+    h = q.Hamiltonian(s, q.xxz_terms(q.chain_bonds(L), 1.0, 1.0))
+    perm, ch = q.translation_group(14)
+    s2 = q.Sector(14, 7, perm).set_irrep(ch[3])
+    h2 = q.Hamiltonian(s2, q.xxz_terms(q.chain_bonds(14) + q.chain_bonds(14, 2), [1.0] * 14 + [0.4] * 14, 0.8))
+    for hh, kw in ((h, dict(mode=A.MODE_FP64, max_iter=150, tol=0.0, reorth=2, seed=20261203)),
+                   (h2, dict(mode=A.MODE_FP64, tol=1e-12, reorth=2)),
+                   (h2, dict(mode=A.MODE_MIXED, tol=1e-12, reorth=2))):
+        monkeypatch.delenv("QMB_REORTH_ALWAYS", raising=False)
+        r1 = hh.lanczos(**kw)
+        monkeypatch.setenv("QMB_REORTH_ALWAYS", "1")
+        r2 = hh.lanczos(**kw)
+        assert abs(r1.E0 - r2.E0) <= 1e-12 * abs(r2.E0), (r1.E0, r2.E0)
+        assert r1.residual <= 10 * r2.residual + 1e-12 * abs(r2.E0)
+    assert abs(r1.E0 - h2.lanczos(mode=A.MODE_FP64, tol=1e-12).E0) <= 1e-10 * abs(r1.E0)
+
+
 def test_matrix_free_solve_matches_stored():
     L, k = 16, 8
     perm, ch = q.translation_group(L)

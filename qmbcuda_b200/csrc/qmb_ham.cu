@@ -337,6 +337,7 @@ __device__ __forceinline__ uint64_t val_key(double v) { return (uint64_t)__doubl
 __device__ __forceinline__ bool val_zero(float v) { return v == 0.0f; }
 __device__ __forceinline__ bool val_zero(double v) { return v == 0.0; }
 __device__ __forceinline__ bool val_zero(float2 v) { return v.x == 0.0f && v.y == 0.0f; }
+__device__ __forceinline__ bool val_zero(double2 v) { return v.x == 0.0 && v.y == 0.0; }
 
 // Every stride-th slot of the sliced ELL's FP32 values (dictionary sample).
 template <class M>
@@ -566,6 +567,105 @@ static void build_cb_t(qmb_ham_s* h, int forced_shift, bool single, CbLayout& L)
     QMB_CUDA_TRY(cudaDeviceSynchronize());
 }
 
+// The FP64 values of a matrix whose FP32 values are coded: when every FP32
+// code stands for one FP64 value (and no FP64 value rounds to an FP32 zero),
+// the FP64 products read the same packed entries through an FP64 dictionary
+// of their own, so the FP64 coded layout costs no entry memory.
+constexpr unsigned long long kDictEmpty = 0x7ff4dead0000beefull;  // a NaN pattern
+template <class M32, class M64>
+__global__ void k_cb_dict64(SellOp<M32> a, const M64* __restrict__ val64, const uint64_t* __restrict__ keys,
+                            int n_keys, unsigned long long* __restrict__ dict_bits, int* __restrict__ bad) {
+    __shared__ uint64_t sk[256];
+    for (int i = threadIdx.x; i < n_keys; i += blockDim.x) sk[i] = keys[i];
+    __syncthreads();
+    constexpr int W = (int)(sizeof(M64) / 8);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.n;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = r >> 5;
+        const int lane = (int)(r & 31);
+        const int w = a.width[s];
+        for (int j = 0; j < w; ++j) {
+            const int64_t k = a.off[s] + (int64_t)j * 32 + lane;
+            const M32 v = a.val[k];
+            const M64 v64 = val64[k];
+            if (val_zero(v)) {
+                if (!val_zero(v64)) atomicExch(bad, 1);
+                continue;
+            }
+            const uint64_t key = val_key(v);
+            int lo = 0, hi = n_keys;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (sk[mid] < key) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo == n_keys || sk[lo] != key) {
+                atomicExch(bad, 1);
+                continue;
+            }
+            const unsigned long long* vb = reinterpret_cast<const unsigned long long*>(&v64);
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+                const unsigned long long prev = atomicCAS(dict_bits + (lo + 1) * W + q, kDictEmpty, vb[q]);
+                if (prev != kDictEmpty && prev != vb[q]) atomicExch(bad, 1);
+            }
+        }
+    }
+}
+
+template <class M32, class M64>
+static void share_cb64_t(qmb_ham_s* h) {
+    const CbLayout& L32 = h->cb32;
+    const int n_keys = L32.n_codes;
+    std::vector<M32> d32(256);
+    QMB_CUDA_TRY(cudaMemcpy(d32.data(), L32.dict.p, 256 * sizeof(M32), cudaMemcpyDeviceToHost));
+    std::vector<uint64_t> keys(n_keys);
+    for (int i = 0; i < n_keys; ++i) {
+        uint64_t k = 0;
+        std::memcpy(&k, &d32[i + 1], sizeof(M32));  // the bits val_key() reads: x low, y high
+        keys[i] = k;
+    }
+    constexpr int W = (int)(sizeof(M64) / 8);
+    DevBuf<uint64_t> dkeys(std::max(1, n_keys));
+    dkeys.upload(keys.data(), n_keys);
+    std::vector<unsigned long long> hb(256 * W, kDictEmpty);
+    DevBuf<unsigned long long> bits(256 * W);
+    bits.upload(hb.data(), hb.size());
+    DevBuf<int> bad(1);
+    bad.zero();
+    SellOp<M32> a = h->sell<M32>(false);
+    k_cb_dict64<M32, M64><<<grid_for(h->n, 256), 256>>>(a, reinterpret_cast<const M64*>(h->val64.p), dkeys.p,
+                                                         n_keys, bits.p, bad.p);
+    check_launch("k_cb_dict64");
+    int hbad = 0;
+    QMB_CUDA_TRY(cudaMemcpy(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hbad) {
+        cb_skip("FP64 values do not map one to one onto the FP32 codes");
+        return;
+    }
+    bits.download(hb.data(), hb.size());
+    QMB_CUDA_TRY(cudaDeviceSynchronize());
+    std::vector<M64> dict(256);
+    std::memset(dict.data(), 0, sizeof(M64) * 256);
+    for (int c = 1; c <= n_keys; ++c)
+        if (hb[(size_t)c * W] != kDictEmpty) std::memcpy(&dict[c], &hb[(size_t)c * W], sizeof(M64));
+    if (L32.nb > 1) {
+        size_t fr = 0, tot = 0;
+        QMB_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        if ((size_t)h->n * sizeof(M64) > fr / 4) {
+            cb_skip("not enough free memory for the FP64 partial sums");
+            return;
+        }
+        h->cb64.ytmp.alloc((size_t)h->n * sizeof(M64));
+    }
+    h->cb64.dict.alloc(256 * sizeof(M64));
+    QMB_CUDA_TRY(cudaMemcpy(h->cb64.dict.p, dict.data(), 256 * sizeof(M64), cudaMemcpyHostToDevice));
+    h->cb64.nb = L32.nb;
+    h->cb64.shift = L32.shift;
+    h->cb64.n_codes = n_keys;
+    h->cb64_shared = true;
+}
+
 //
 // The same layout with one block (every column in the 24-bit field) serves a
 // matrix whose vectors fit L2 but whose entry stream is large (the plain FP32
@@ -595,6 +695,12 @@ void build_cb(qmb_ham_s* h) {
     if ((h->prec & QMB_PREC_FP64) && h->val64.p && !h->cplx && (double)h->n * 8 <= kCbMaxSingleVecBytes &&
         (double)h->padded * 12 >= kCbMinStreamBytes)
         build_cb_t<double>(h, 0, true, h->cb64);
+    // otherwise FP64 values share the FP32 layout's entries where they can
+    const char* se = std::getenv("QMB_CB_SHARE64");
+    if (h->cb64.nb == 0 && h->cb32.nb > 0 && h->val64.p && h->val32.p && !(se && se[0] == '0')) {
+        if (h->cplx) share_cb64_t<float2, double2>(h);
+        else share_cb64_t<float, double>(h);
+    }
 }
 
 // Row-order copies for the matrix-free lookup: each row's representative
@@ -895,7 +1001,8 @@ void hv_dispatch(const qmb_ham_s* h, int prec, const void* x, void* y, cudaStrea
     QMB_REQUIRE(f64 ? h->val64.p != nullptr : h->val32.p != nullptr, QMB_ERR_INVALID,
                 "the handle does not hold values of the requested precision");
     if (h->cplx) {
-        if (f64) launch_hv(h->sell<double2>(true), (const double2*)x, (double2*)y, st, 0);
+        if (f64 && h->cb64.nb > 0) launch_hv(h->cb<double2>(), (const double2*)x, (double2*)y, st, CbSellOp<double2>::smem_bytes());
+        else if (f64) launch_hv(h->sell<double2>(true), (const double2*)x, (double2*)y, st, 0);
         else if (h->cb32.nb > 0) launch_hv(h->cb<float2>(), (const float2*)x, (float2*)y, st, CbSellOp<float2>::smem_bytes());
         else launch_hv(h->sell<float2>(false), (const float2*)x, (float2*)y, st, 0);
     } else {

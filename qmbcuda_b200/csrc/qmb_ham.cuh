@@ -788,6 +788,7 @@ struct qmb_ham_s {
     // coded layouts of the stored values (CbSellOp): FP32 (column-blocked for
     // vectors larger than L2, else one block) and real FP64 (one block)
     qmb::CbLayout cb32, cb64;
+    bool cb64_shared = false;  // cb64 reads cb32's packed entries (its own dictionary and partial sums)
     // terms kept for the matrix-free operator
     int n_terms = 0, n_col = 0;
     qmb::DevBuf<int> t_nops;
@@ -856,14 +857,15 @@ struct qmb_ham_s {
     template <class M> qmb::CbSellOp<M> cb() const {
         constexpr bool f64 = sizeof(typename qmb::Sc<M>::real) == 8;
         const qmb::CbLayout& L = f64 ? cb64 : cb32;
+        const qmb::CbLayout& E = (f64 && cb64_shared) ? cb32 : L;  // where the entries live
         qmb::CbSellOp<M> op;
         op.n = n;
         op.nb = L.nb;
         op.shift = L.shift;
         op.n_slices = n_slices;
-        op.off = L.off.p;
-        op.width = L.width.p;
-        op.packed = L.packed.p;
+        op.off = E.off.p;
+        op.width = E.width.p;
+        op.packed = E.packed.p;
         op.dict = reinterpret_cast<const M*>(L.dict.p);
         op.diag = reinterpret_cast<const M*>(f64 ? diag64.p : diag32.p);
         op.ytmp = L.ytmp.p;

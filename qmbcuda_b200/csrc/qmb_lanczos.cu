@@ -907,11 +907,9 @@ extern "C" qmb_status qmb_lanczos(qmb_ham h, const qmb_lanczos_opts* opts, qmb_l
                 else k(h->sell<R>(false), (size_t)0);
             };
             auto op64 = [&](auto&& k) {
-                if constexpr (std::is_same<D, double>::value) {
-                    if (h->cb64.nb > 0) {
-                        k(h->cb<D>(), CbSellOp<D>::smem_bytes());
-                        return;
-                    }
+                if (h->cb64.nb > 0) {
+                    k(h->cb<D>(), CbSellOp<D>::smem_bytes());
+                    return;
                 }
                 k(h->sell<D>(true), (size_t)0);
             };

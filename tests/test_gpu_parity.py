@@ -285,8 +285,10 @@ def test_column_blocked_product_and_solve(a, monkeypatch):
     """The column-blocked coded FP32 layout (built for vectors larger than L2;
     QMB_CB_SHIFT=10 forces 1024-row blocks here): the FP32 product equals the
     oracle's matrix product to FP32 rounding and the plain sliced-ELL product
-    to 2e-6 relative, and a mixed and an FP32 solve on it match the oracle's
-    FP64 ground energy (scipy eigsh)."""
+    to 2e-6 relative; the FP64 values share its packed entries through an
+    FP64 dictionary, and the FP64 product matches the oracle to 1e-12; mixed,
+    FP64 and FP32 solves on it match the oracle's FP64 ground energy (scipy
+    eigsh)."""
     import torch
     L, k = 20, 10
     perm, ch = q.translation_group(L)
@@ -317,8 +319,21 @@ def test_column_blocked_product_and_solve(a, monkeypatch):
     scale = np.abs(want).max()
     assert np.abs(got - want).max() <= 2e-6 * scale
     assert np.abs(got - y2.cpu().numpy()).max() <= 2e-6 * scale
+    # the FP64 values share the packed entries through an FP64 dictionary
+    assert hb.info.coded_fp64 == 1
+    dt64 = torch.complex128 if hb.info.is_complex else torch.float64
+    x64 = torch.tensor(xh, dtype=dt64, device="cuda")
+    z1, z2 = torch.empty_like(x64), torch.empty_like(x64)
+    for h, y in ((hb, z1), (plain, z2)):
+        q.check(q.lib().qmb_hv(h.h, q._capi.PREC_FP64, q._capi.C.c_void_p(x64.data_ptr()), q._capi.C.c_void_p(y.data_ptr()), None))
+    torch.cuda.synchronize()
+    want64 = M @ xh
+    assert np.abs(z1.cpu().numpy() - want64).max() <= 1e-12 * np.abs(want64).max()
+    assert np.abs(z1.cpu().numpy() - z2.cpu().numpy()).max() <= 1e-12 * np.abs(want64).max()
     e = O.ground_energy_sparse(M)
     r = hb.lanczos(mode=q._capi.MODE_MIXED, tol=1e-12)
     assert abs(r.E0 - e) <= 1e-10 * abs(e), (r.E0, e)
+    r64 = hb.lanczos(mode=q._capi.MODE_FP64, tol=1e-12)
+    assert abs(r64.E0 - e) <= 1e-10 * abs(e), (r64.E0, e)
     r32 = hb.lanczos(mode=q._capi.MODE_FP32, tol=1e-12, allow_unconverged=True)
     assert abs(r32.E0 - e) <= 1e-5 * abs(e), (r32.E0, e)

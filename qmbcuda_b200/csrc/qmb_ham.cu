@@ -806,9 +806,14 @@ void mf_tables(qmb_ham_s* h) {
     while (ibits < 63 && ((n - 1) >> ibits)) ++ibits;
     const char* he = std::getenv("QMB_MF_HASH");
     const bool force_hash = he && he[0] == '1';
-    if (!r32 && (force_hash || (double)n * 8 >= kMfHashMinBytes) && bits + ibits <= 63) {
-        uint64_t slots = 1;
-        while (slots < 2 * (uint64_t)n) slots <<= 1;
+    uint64_t slots = 1;
+    while (slots < 2 * (uint64_t)n) slots <<= 1;
+    size_t fr = 0, tot = 0;
+    QMB_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    // the table is an accelerator: without room for it (a quarter of the
+    // free memory) the bucket search serves alone
+    if (!r32 && (force_hash || (double)n * 8 >= kMfHashMinBytes) && bits + ibits <= 63 &&
+        slots * sizeof(uint64_t) <= fr / 4) {
         h->mf_hash.alloc(slots);
         QMB_CUDA_TRY(cudaMemset(h->mf_hash.p, 0xff, slots * sizeof(uint64_t)));
         h->mf_hmask = slots - 1;
